@@ -1,0 +1,314 @@
+"""ctypes binding of the FP64 CPU oracle (oracle/cy3_oracle.cpp).
+
+TEST INFRASTRUCTURE ONLY.  Imported by tests/, by ``__graft_entry__.smoke()`` and by the
+CPU-baseline leg of ``bench.py`` -- never by the product package ``papers_b200``.
+
+The oracle restates the reference crate ``substrate_sm_derivation/cy3_solver`` (Rust) function
+by function; each wrapper below names the reference function it mirrors.  ``OracleSolver``
+mirrors the reference workspace ``QuinticSolver`` (src/quintic.rs:117-165) so tests read like
+the reference's own tests.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "liboracle.so")
+_lib = None
+
+_dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_up = np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")
+_ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+
+
+def build(force: bool = False) -> str:
+    """Compile liboracle.so with the committed Makefile (gcc, -ffp-contract=off)."""
+    if force or not os.path.exists(_LIB_PATH) or os.path.getmtime(_LIB_PATH) < os.path.getmtime(
+        os.path.join(_HERE, "cy3_oracle.cpp")
+    ):
+        subprocess.check_call(["make", "-s", "-C", _HERE, "liboracle.so"])
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(_LIB_PATH):
+        build()
+    L = C.CDLL(_LIB_PATH)
+    sz = C.c_size_t
+    d = C.c_double
+    L.orc_set_threads.argtypes = [C.c_int]
+    L.orc_get_threads.restype = C.c_int
+    L.orc_quintic_value.argtypes = [_dp, d, d, _dp]
+    L.orc_quintic_gradient.argtypes = [_dp, d, d, _dp]
+    L.orc_lcg_normals.argtypes = [C.c_uint64, sz, _dp]
+    L.orc_lcg_uniforms.argtypes = [C.c_uint64, sz, _dp]
+    L.orc_sample_sz.argtypes = [sz, C.c_uint64, d, d, C.c_int, C.c_int, C.c_int, _dp, C.POINTER(sz)]
+    L.orc_sample_sz.restype = sz
+    L.orc_sample_newton.argtypes = [sz, C.c_uint64, d, d, C.c_int, d, _dp]
+    L.orc_sample_newton.restype = sz
+    L.orc_weights.argtypes = [_dp, sz, d, d, _dp]
+    L.orc_log_omega.argtypes = [_dp, sz, d, d, _dp, _ip, _ip]
+    L.orc_monomials.argtypes = [C.c_int, C.c_int, C.c_void_p]
+    L.orc_monomials.restype = C.c_int
+    L.orc_basis.argtypes = [_dp, sz, _up, C.c_int, _dp]
+    L.orc_basis_derivs.argtypes = [_dp, sz, _up, C.c_int, _dp]
+    L.orc_fs_gram_matrix.argtypes = [_dp, _dp, sz, C.c_int, _dp, _dp]
+    L.orc_cholesky.argtypes = [_dp, _dp, C.c_int, _dp, _dp]
+    L.orc_cholesky.restype = C.c_int
+    L.orc_fs_gram_orthonormalise.argtypes = [_dp, C.c_void_p, _dp, sz, C.c_int]
+    L.orc_fs_gram_orthonormalise.restype = C.c_int
+    L.orc_invert_real.argtypes = [_dp, C.c_int, _dp]
+    L.orc_invert_real.restype = C.c_int
+    L.orc_inv_k.argtypes = [_dp, sz, C.c_int, _dp, _dp]
+    L.orc_t_operator.argtypes = [_dp, _dp, sz, C.c_int, _dp, _dp, C.c_void_p, C.c_void_p]
+    L.orc_donaldson_step.argtypes = [_dp, _dp, sz, C.c_int, _dp, C.POINTER(d)]
+    L.orc_donaldson_step.restype = C.c_int
+    L.orc_sigma.argtypes = [_dp, _dp, _dp, _dp, _dp, sz, C.c_int, d, d, _dp, C.c_void_p]
+    L.orc_sigma.restype = d
+    L.orc_point_grad.argtypes = [_dp, _dp, _dp, _dp, d, C.c_int, d, d, _dp, C.POINTER(d), C.POINTER(d)]
+    L.orc_sigma_grad.argtypes = [_dp, _dp, _dp, _dp, _dp, sz, C.c_int, d, d, _dp, C.POINTER(d), _dp, C.POINTER(d)]
+    L.orc_sigma_grad.restype = C.c_int
+    L.orc_adam_refine.argtypes = [_dp, _dp, _dp, _dp, _dp, sz, C.c_int, d, d, _dp, C.c_int, d, d, d, d, _dp]
+    L.orc_adam_refine.restype = C.c_int
+    _lib = L
+    return L
+
+
+def set_threads(n: int) -> None:
+    lib().orc_set_threads(int(n))
+
+
+def threads() -> int:
+    return int(lib().orc_get_threads())
+
+
+# ---------------------------------------------------------------------------------------------
+# free functions
+# ---------------------------------------------------------------------------------------------
+def quintic_value(z: np.ndarray, psi: complex = 0.0) -> complex:
+    """deformed_fermat_quintic (quintic.rs:3248) at one point z [10]."""
+    psi = complex(psi)
+    out = np.empty(2)
+    lib().orc_quintic_value(np.ascontiguousarray(z, dtype=np.float64), psi.real, psi.imag, out)
+    return complex(out[0], out[1])
+
+
+def quintic_gradient(z: np.ndarray, psi: complex = 0.0) -> np.ndarray:
+    """deformed_fermat_quintic_gradient (quintic.rs:3276): 10 reals."""
+    psi = complex(psi)
+    out = np.empty(10)
+    lib().orc_quintic_gradient(np.ascontiguousarray(z, dtype=np.float64), psi.real, psi.imag, out)
+    return out
+
+
+def lcg_normals(seed: int, n: int) -> np.ndarray:
+    """LCG(seed).next_normal() stream (src/lib.rs:225-246)."""
+    out = np.empty(n)
+    lib().orc_lcg_normals(seed, n, out)
+    return out
+
+
+def lcg_uniforms(seed: int, n: int) -> np.ndarray:
+    out = np.empty(n)
+    lib().orc_lcg_uniforms(seed, n, out)
+    return out
+
+
+def sample_sz(n: int, seed: int, psi: complex = 0.0, fermat_variant: bool = True, dk_iters: int = 50,
+              newton_iters: int = 0):
+    """Line-intersection sampler: sample_quintic_points_sz (quintic.rs:3633) when fermat_variant,
+    else sample_deformed_quintic_points_sz (quintic.rs:3810) with complex psi.
+    Returns (points [P,10], lines_tried)."""
+    out = np.empty((n, 10))
+    tried = C.c_size_t(0)
+    psi = complex(psi)
+    got = lib().orc_sample_sz(n, seed, psi.real, psi.imag, 0 if fermat_variant else 1, dk_iters, newton_iters,
+                              out.reshape(-1), C.byref(tried))
+    return np.ascontiguousarray(out[:got]), int(tried.value)
+
+
+def sample_newton(n: int, seed: int, psi: complex = 0.0, fermat_variant: bool = True, tol: float = 1e-12):
+    """Newton-projection sampler (quintic.rs:3568 / 3448)."""
+    out = np.empty((n, 10))
+    psi = complex(psi)
+    got = lib().orc_sample_newton(n, seed, psi.real, psi.imag, 0 if fermat_variant else 1, tol, out.reshape(-1))
+    return np.ascontiguousarray(out[:got])
+
+
+def weights(pts: np.ndarray, psi: complex = 0.0) -> np.ndarray:
+    """cy_measure_weights(_psi) (quintic.rs:3507-3563)."""
+    psi = complex(psi)
+    w = np.empty(len(pts))
+    lib().orc_weights(np.ascontiguousarray(pts).reshape(-1), len(pts), psi.real, psi.imag, w)
+    return w
+
+
+def log_omega(pts: np.ndarray, psi: complex = 0.0):
+    """log|Omega|^2, chart, elim (quintic.rs:4858-4916). Returns (log_om, chart, elim)."""
+    psi = complex(psi)
+    P = len(pts)
+    lo = np.empty(P)
+    ch = np.empty(P, np.int32)
+    el = np.empty(P, np.int32)
+    lib().orc_log_omega(np.ascontiguousarray(pts).reshape(-1), P, psi.real, psi.imag, lo, ch, el)
+    return lo, ch, el
+
+
+def monomials(k: int, reduced: bool = False) -> np.ndarray:
+    """build_degree_k_quintic_monomials (quintic.rs:3192); reduced drops e0 >= 5."""
+    n = lib().orc_monomials(k, int(reduced), None)
+    out = np.empty((n, 5), np.uint32)
+    lib().orc_monomials(k, int(reduced), out.ctypes.data)
+    return out
+
+
+def basis(pts: np.ndarray, mono: np.ndarray) -> np.ndarray:
+    """evaluate_quintic_basis (quintic.rs:4021): [P, 2N] interleaved (re, im)."""
+    P, N = len(pts), len(mono)
+    s = np.empty((P, 2 * N))
+    lib().orc_basis(np.ascontiguousarray(pts).reshape(-1), P, np.ascontiguousarray(mono).reshape(-1), N, s.reshape(-1))
+    return s
+
+
+def basis_derivs(pts: np.ndarray, mono: np.ndarray) -> np.ndarray:
+    """evaluate_quintic_basis_derivs_soa (quintic.rs:1231): [P, 5, 2N]."""
+    P, N = len(pts), len(mono)
+    d = np.empty((P, 5, 2 * N))
+    lib().orc_basis_derivs(np.ascontiguousarray(pts).reshape(-1), P, np.ascontiguousarray(mono).reshape(-1), N,
+                           d.reshape(-1))
+    return d
+
+
+def fs_gram_matrix(s: np.ndarray, w: np.ndarray):
+    """compute_fs_gram_matrix (quintic.rs:2957)."""
+    P, N = s.shape[0], s.shape[1] // 2
+    gr = np.empty((N, N))
+    gi = np.empty((N, N))
+    lib().orc_fs_gram_matrix(s.reshape(-1), w, P, N, gr.reshape(-1), gi.reshape(-1))
+    return gr, gi
+
+
+def invert_real(a: np.ndarray) -> np.ndarray:
+    n = a.shape[0]
+    out = np.empty_like(a)
+    rc = lib().orc_invert_real(np.ascontiguousarray(a).reshape(-1), n, out.reshape(-1))
+    if rc != 0:
+        raise np.linalg.LinAlgError("singular")
+    return out
+
+
+def t_operator(s: np.ndarray, w: np.ndarray, h_block: np.ndarray) -> np.ndarray:
+    """Trace-renormalised lower-index T(h) packed as a 2N x 2N block (quintic.rs:1761-1826)."""
+    P, N = s.shape[0], s.shape[1] // 2
+    tb = np.empty((2 * N, 2 * N))
+    lib().orc_t_operator(s.reshape(-1), w, P, N, np.ascontiguousarray(h_block).reshape(-1), tb.reshape(-1), None, None)
+    return tb
+
+
+def identity_h(N: int) -> np.ndarray:
+    """init_h_block_identity (quintic.rs:4120)."""
+    return np.eye(2 * N)
+
+
+# ---------------------------------------------------------------------------------------------
+# QuinticSolver mirror
+# ---------------------------------------------------------------------------------------------
+class OracleSolver:
+    """Mirror of the reference workspace `QuinticSolver` (quintic.rs:117-165) on the oracle."""
+
+    def __init__(self, points, weights_, log_om, monomials_, psi=0.0, k_degree=None):
+        self.points = np.ascontiguousarray(points, dtype=np.float64)
+        self.n_points = len(self.points)
+        self.weights = np.ascontiguousarray(weights_, dtype=np.float64)
+        self.log_omega_sq = np.ascontiguousarray(log_om, dtype=np.float64)
+        self.monomials = np.ascontiguousarray(monomials_, dtype=np.uint32)
+        self.n_basis = len(self.monomials)
+        self.k_degree = k_degree
+        self.psi = complex(psi)
+        self.section_values = basis(self.points, self.monomials)
+        self.section_derivs = basis_derivs(self.points, self.monomials)
+        self.h_block = identity_h(self.n_basis)
+        self.donaldson_residuals: list[float] = []
+
+    # constructors (quintic.rs:174-322)
+    @classmethod
+    def new_with_sampler(cls, k, n_points, seed, newton_tol=1e-12, sampler="sz", reduced=False):
+        """QuinticSolver::new_with_sampler (quintic.rs:281), Fermat quintic."""
+        if sampler == "sz":
+            pts, _ = sample_sz(n_points, seed, 0.0, fermat_variant=True)
+        else:
+            pts = sample_newton(n_points, seed, 0.0, True, newton_tol)
+        if len(pts) == 0:
+            return None
+        lo, _, _ = log_omega(pts, 0.0)
+        return cls(pts, weights(pts, 0.0), lo, monomials(k, reduced), 0.0, k)
+
+    @classmethod
+    def new_with_psi_sz(cls, k, n_points, seed, psi, reduced=False, newton_iters=0):
+        """QuinticSolver::new_with_psi_sz (quintic.rs:240), extended to complex psi."""
+        pts, _ = sample_sz(n_points, seed, psi, fermat_variant=False, newton_iters=newton_iters)
+        if len(pts) == 0:
+            return None
+        lo, _, _ = log_omega(pts, psi)
+        return cls(pts, weights(pts, psi), lo, monomials(k, reduced), psi, k)
+
+    # methods
+    def orthonormalise_basis_fs_gram(self):
+        """quintic.rs:3140."""
+        rc = lib().orc_fs_gram_orthonormalise(self.section_values.reshape(-1), self.section_derivs.ctypes.data,
+                                              self.weights, self.n_points, self.n_basis)
+        if rc != 0:
+            raise ValueError("FS Gram matrix not positive-definite")
+        self.h_block = identity_h(self.n_basis)
+
+    def donaldson_step(self) -> float:
+        """quintic.rs:428 -> donaldson_step_workspace (quintic.rs:1734)."""
+        r = C.c_double(0.0)
+        lib().orc_donaldson_step(self.section_values.reshape(-1), self.weights, self.n_points, self.n_basis,
+                                 self.h_block.reshape(-1), C.byref(r))
+        return r.value
+
+    def donaldson_solve(self, max_iter: int, tol: float) -> int:
+        """quintic.rs:433."""
+        self.donaldson_residuals = []
+        for _ in range(max_iter):
+            r = self.donaldson_step()
+            self.donaldson_residuals.append(r)
+            if r < tol:
+                break
+        return len(self.donaldson_residuals)
+
+    def sigma(self, return_eta: bool = False):
+        """quintic.rs:423 -> compute_sigma_from_workspace (quintic.rs:1301)."""
+        eta = np.empty(self.n_points)
+        v = lib().orc_sigma(self.section_values.reshape(-1), self.section_derivs.reshape(-1), self.points.reshape(-1),
+                            self.log_omega_sq, self.weights, self.n_points, self.n_basis, self.psi.real,
+                            self.psi.imag, self.h_block.reshape(-1), eta.ctypes.data)
+        return (v, eta) if return_eta else v
+
+    def sigma_squared_and_gradient(self):
+        """sigma_squared_and_gradient (quintic.rs:2714): (sigma_L2^2, grad[2N^2], sigma_L1)."""
+        n = self.n_basis
+        g = np.empty(2 * n * n)
+        l2 = C.c_double()
+        l1 = C.c_double()
+        lib().orc_sigma_grad(self.section_values.reshape(-1), self.section_derivs.reshape(-1), self.points.reshape(-1),
+                             self.log_omega_sq, self.weights, self.n_points, n, self.psi.real, self.psi.imag,
+                             self.h_block.reshape(-1), C.byref(l2), g, C.byref(l1))
+        return l2.value, g, l1.value
+
+    def sigma_refine_analytic(self, n_iter: int, lr: float, beta1=0.9, beta2=0.999, eps=1e-8):
+        """QuinticSolver::sigma_refine_analytic (quintic.rs:453)."""
+        hist = np.empty(max(n_iter, 1))
+        done = lib().orc_adam_refine(self.section_values.reshape(-1), self.section_derivs.reshape(-1),
+                                     self.points.reshape(-1), self.log_omega_sq, self.weights, self.n_points,
+                                     self.n_basis, self.psi.real, self.psi.imag, self.h_block.reshape(-1), n_iter, lr,
+                                     beta1, beta2, eps, hist)
+        return list(hist[:done])
