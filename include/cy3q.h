@@ -1,0 +1,191 @@
+/*
+ * cy3q.h -- C ABI of the B200 (sm_100a) CY3 quintic metric solver.
+ *
+ * Drop-in boundary for the data-parallel hot path of the reference crate
+ * `substrate_sm_derivation/cy3_solver` (Rust).  The reference exposes that path as the
+ * in-process Rust workspace `QuinticSolver` (src/quintic.rs:117-165) plus free functions and the
+ * GPU object `AdamGradientKernel` (src/gpu_adam.rs:1533-2195).  Each entry point below names the
+ * reference interface it replaces.  All arrays are caller-owned HOST memory in the reference's
+ * layouts, copied in and out; device state is owned by the handle.  Plain C types only.
+ *
+ * Layouts (reference conventions):
+ *   points      [P x 10]  f64, (re, im) of z_0..z_4 interleaved            (quintic.rs:128)
+ *   weights     [P]       f64, w_p = 1/|grad f|^2                          (quintic.rs:3507)
+ *   log_omega   [P]       f64, log|Omega|^2                                (quintic.rs:4858)
+ *   h_block     [2N x 2N] f64 row-major, [2a][2b] = Re h_ab, [2a][2b+1] = -Im h_ab,
+ *                         [2a+1][2b] = Im h_ab, [2a+1][2b+1] = Re h_ab       (quintic.rs:4081-4085)
+ *   grad        [2N^2]    f64, first N^2 = d/d Re h_ab, next N^2 = d/d Im h_ab (quintic.rs:2306-2308)
+ *   monomials   [N x 5]   u32 exponents, lex order with e0 outermost       (quintic.rs:3192)
+ *
+ * Threading: a solver handle is single-threaded (the reference methods take &mut self).
+ * The server handle (cy3q_server_*) is thread-safe.  No function throws or aborts across the
+ * ABI; failures return a status and leave a message for cy3q_last_error().
+ */
+#ifndef CY3Q_H
+#define CY3Q_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  CY3Q_OK = 0,
+  CY3Q_ERR_ARG = 1,          /* bad argument (null pointer, out-of-range value) */
+  CY3Q_ERR_SHAPE = 2,        /* size mismatch or size beyond a stated limit */
+  CY3Q_ERR_CUDA = 3,         /* CUDA runtime / library error */
+  CY3Q_ERR_OOM = 4,          /* device allocation failed or HBM budget exceeded */
+  CY3Q_ERR_SINGULAR = 5,     /* T-operator not invertible (the reference silently sets h = I, quintic.rs:1874) */
+  CY3Q_ERR_NONFINITE = 6,    /* NaN / Inf in an input or a result */
+  CY3Q_ERR_TIMEOUT = 7,      /* deadline passed (server wait, device watchdog) */
+  CY3Q_ERR_CANCELLED = 8,    /* request cancelled */
+  CY3Q_ERR_UNSUPPORTED = 9,  /* option not supported by this build */
+  CY3Q_ERR_NOT_PD = 10,      /* FS Gram matrix not positive-definite (quintic.rs:3148-3149) */
+  CY3Q_ERR_EMPTY = 11        /* no sample points (the reference constructors return None, quintic.rs:204) */
+} cy3q_status;
+
+typedef enum {
+  CY3Q_SAMPLER_NEWTON = 0,   /* SamplerKind::NewtonProjection (quintic.rs:3613) */
+  CY3Q_SAMPLER_SZ = 1        /* SamplerKind::ShiffmanZelditch: line intersection (quintic.rs:3633, 3810) */
+} cy3q_sampler;
+
+typedef enum {
+  CY3Q_PREC_FP64 = 0,        /* FP64 everywhere: the drop-in, parity 1e-10 with the FP64 reference path */
+  CY3Q_PREC_FP16X3 = 1,      /* split-precision tcgen05 GEMMs: fp16 hi/lo operands, 3 products, FP32 TMEM
+                                accumulation flushed to FP64; FP64 inverse, log-det and reductions */
+  CY3Q_PREC_BF16X3 = 2       /* same with bf16 hi/lo operands */
+} cy3q_precision;
+
+typedef struct {
+  uint32_t k;                /* section degree k (quintic.rs:120) */
+  double psi_re, psi_im;     /* psi of f = sum z^5 - 5 psi prod z; the reference takes a real psi (quintic.rs:125) */
+  uint64_t n_points;         /* requested sample points */
+  uint64_t seed;             /* LCG seed (lib.rs:225) */
+  int32_t sampler;           /* cy3q_sampler */
+  int32_t fermat_variant;    /* 1: sample_quintic_points_sz (Fermat f, |f|<=1e-3, 4x lines, quintic.rs:3633);
+                                0: sample_deformed_quintic_points_sz (psi f, |f|<=1e-2, 8x lines, quintic.rs:3810) */
+  int32_t dk_iters;          /* Durand-Kerner sweeps per line (reference: 50, quintic.rs:250) */
+  int32_t newton_polish;     /* FP64 Newton steps on each root after Durand-Kerner (0 = reference behaviour) */
+  int32_t reduced_basis;     /* 1: drop monomials divisible by z0^5 (ideal-reduced basis, N_6 = 205, N_8 = 460) */
+  int32_t precision;         /* cy3q_precision */
+  int32_t with_derivs;       /* 1: keep section derivatives resident (needed for sigma / gradient / Laplacian) */
+  int32_t device;            /* CUDA device ordinal */
+  uint64_t hbm_budget_bytes; /* 0 = no limit; allocations beyond it fail with CY3Q_ERR_OOM */
+  double newton_tol;         /* Newton-projection sampler tolerance (quintic.rs:174) */
+} cy3q_config;
+
+typedef struct cy3q_solver cy3q_solver;
+
+/* ---- lifecycle: QuinticSolver::new / new_with_psi / new_with_psi_sz / new_with_sampler (quintic.rs:174-322) ---- */
+cy3q_status cy3q_config_default(cy3q_config* cfg);
+cy3q_status cy3q_solver_create(const cy3q_config* cfg, cy3q_solver** out);
+void cy3q_solver_destroy(cy3q_solver* s);
+/* Copies the last error message of the handle (or of the calling thread when s == NULL). */
+cy3q_status cy3q_last_error(const cy3q_solver* s, char* buf, size_t len);
+/* Use a caller-provided CUDA stream (cudaStream_t passed as void*); NULL restores the handle's own stream. */
+cy3q_status cy3q_set_stream(cy3q_solver* s, void* cuda_stream);
+cy3q_status cy3q_set_precision(cy3q_solver* s, int32_t precision);
+
+/* ---- sample set ---- */
+/* GPU line-intersection / Newton sampler + weights + log|Omega|^2 + section tables
+   (sample_quintic_points_with quintic.rs:4006, cy_measure_weights quintic.rs:3507,
+   finish_workspace_construction quintic.rs:328).  Resets h to identity. */
+cy3q_status cy3q_sample(cy3q_solver* s);
+/* Install caller points (identical-point parity runs).  w / log_omega may be NULL: then they are
+   computed on the device from the points (quintic.rs:3507-3563, 4858). Resets h to identity. */
+cy3q_status cy3q_set_points(cy3q_solver* s, const double* points, const double* weights, const double* log_omega,
+                            uint64_t n_points);
+cy3q_status cy3q_get_points(const cy3q_solver* s, double* points, double* weights, double* log_omega);
+cy3q_status cy3q_n_points(const cy3q_solver* s, uint64_t* n);
+cy3q_status cy3q_n_basis(const cy3q_solver* s, uint32_t* n);
+cy3q_status cy3q_get_basis(const cy3q_solver* s, uint32_t* monomials);
+/* Section values s [P x 2N] (evaluate_quintic_basis, quintic.rs:4021) in the current basis. */
+cy3q_status cy3q_get_sections(const cy3q_solver* s, double* section_values);
+
+/* ---- balancing: QuinticSolver::orthonormalise_basis_fs_gram / donaldson_step / donaldson_solve ---- */
+cy3q_status cy3q_orthonormalise_fs_gram(cy3q_solver* s);                             /* quintic.rs:3140 */
+cy3q_status cy3q_donaldson_step(cy3q_solver* s, double* residual);                   /* quintic.rs:428, 1734 */
+/* quintic.rs:433; residual_trace may be NULL, else holds max_iter entries. */
+cy3q_status cy3q_donaldson_solve(cy3q_solver* s, int32_t max_iter, double tol, int32_t* iters,
+                                 double* residual_trace);
+cy3q_status cy3q_get_h(const cy3q_solver* s, double* h_block);
+cy3q_status cy3q_set_h(cy3q_solver* s, const double* h_block);
+
+/* ---- sigma functional (compute_sigma_from_workspace quintic.rs:1301) ---- */
+cy3q_status cy3q_sigma(cy3q_solver* s, double* sigma_l1);
+/* Per-point eta (NaN for skipped points) of the last cy3q_sigma call, [P]. */
+cy3q_status cy3q_get_eta(const cy3q_solver* s, double* eta);
+/* sigma on other points with the current h (C1: fresh points, seed 0); w / log_omega may be NULL. */
+cy3q_status cy3q_sigma_on_points(cy3q_solver* s, const double* points, const double* weights,
+                                 const double* log_omega, uint64_t n_points, double* sigma_l1);
+/* sigma_squared_and_gradient (quintic.rs:2714) / AdamGradientKernel::compute_sigma_grad_h_only
+   (gpu_adam.rs:1769): sigma_L2^2, gradient [2N^2] and sigma_L1. */
+cy3q_status cy3q_sigma_grad(cy3q_solver* s, double* sigma_l2sq, double* grad, double* sigma_l1);
+/* QuinticSolver::sigma_refine_analytic (quintic.rs:453) with optional minibatching: minibatch == 0 or
+   >= P uses every point (the reference behaviour); otherwise each step draws `minibatch` points by a
+   seeded permutation.  history[steps] receives sigma_L1 before each update; *steps_done the count. */
+cy3q_status cy3q_adam_refine(cy3q_solver* s, int32_t steps, double lr, uint64_t minibatch, uint64_t seed,
+                             double* history, int32_t* steps_done);
+
+/* ---- Laplacian Galerkin spectrum + Yukawa overlap (templates: route34/metric_laplacian.rs:296-710,
+        route34/yukawa_overlap_real.rs:372) ---- */
+typedef struct {
+  uint32_t test_degree;      /* degree of the sections s in the (d,d) test functions f = s_a conj(s_b) / K^d */
+  uint32_t n_eigs;           /* lowest eigenvalues returned */
+  double reg;                /* relative Tikhonov regularisation of the mass matrix */
+} cy3q_laplacian_config;
+/* Assembles mass and stiffness matrices over the solver's points with the current balanced h and
+   returns the lowest n_eigs eigenvalues of K v = lambda M v (FP64 eigensolve).  eigs [n_eigs]. */
+cy3q_status cy3q_laplacian(cy3q_solver* s, const cy3q_laplacian_config* cfg, double* eigs);
+/* Y_ijk = sum_p w_p psi_i psi_j psi_k conj(Omega_p) / sum_p w_p with psi_i = sum_alpha c_{i,alpha} f_alpha
+   (n_modes x M complex coefficients, interleaved), y [n_modes^3 x 2]. */
+cy3q_status cy3q_yukawa(cy3q_solver* s, const cy3q_laplacian_config* cfg, const double* coeffs, uint32_t n_modes,
+                        double* y);
+
+/* ---- serving: continuous batching of balancing solves on one GPU (no reference analogue; nearest is
+        the toy crossbeam work queue, src/orchestrator.rs:1-120) ---- */
+typedef struct cy3q_server cy3q_server;
+typedef struct {
+  uint32_t k;
+  double psi_re, psi_im;
+  uint64_t n_points;
+  uint64_t seed;
+  int32_t iterations;        /* balancing iterations */
+  int32_t precision;         /* cy3q_precision */
+  int32_t reduced_basis;
+} cy3q_request;
+typedef struct {
+  cy3q_status status;
+  double sigma_l1;           /* sigma after the last iteration (NaN when not requested) */
+  double residual;           /* last balancing residual */
+  int32_t iterations;
+  uint32_t n_basis;
+  double submit_ms, start_ms, finish_ms;   /* times on the server clock */
+} cy3q_result;
+typedef struct {
+  uint64_t submitted, completed, failed, cancelled;
+  double p50_ms, p99_ms;     /* solve latency (submit -> finish) over completed requests */
+  double iters_per_s;        /* aggregate balancing iterations per second since server start */
+  uint64_t hbm_in_use, hbm_peak;
+} cy3q_server_stats;
+
+cy3q_status cy3q_server_create(int32_t device, uint64_t hbm_budget_bytes, int32_t max_active, cy3q_server** out);
+void cy3q_server_destroy(cy3q_server* srv);
+cy3q_status cy3q_submit(cy3q_server* srv, const cy3q_request* req, uint64_t* ticket);
+cy3q_status cy3q_wait(cy3q_server* srv, uint64_t ticket, int64_t timeout_ms, cy3q_result* out);
+cy3q_status cy3q_cancel(cy3q_server* srv, uint64_t ticket);
+cy3q_status cy3q_server_stats_get(cy3q_server* srv, cy3q_server_stats* out);
+/* h of a completed request, [2N x 2N] in the reference packing. */
+cy3q_status cy3q_result_h(cy3q_server* srv, uint64_t ticket, double* h_block);
+
+/* ---- build / device information ---- */
+const char* cy3q_version(void);
+/* Number of this library's kernels launched by the handle since the last reset. */
+cy3q_status cy3q_launch_count(const cy3q_solver* s, uint64_t* launches, int32_t reset);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CY3Q_H */

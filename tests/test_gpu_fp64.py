@@ -1,0 +1,163 @@
+"""GPU parity of the FP64 drop-in path (CY3Q_PREC_FP64) against the FP64 oracle, through the C ABI.
+
+Tolerances (north star: the FP64 Donaldson iteration must match the reference FP64 CPU path on
+identical points to relative Frobenius error 1e-10 on h and 1e-10 on sigma):
+  * h_block after n balancing steps: ||h_gpu - h_orc||_F / ||h_orc||_F <= 1e-10
+  * sigma_L1 (and eta per point):    relative error <= 1e-10
+  * gradient of sigma_L2^2:          relative Frobenius error <= 1e-9
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+GOLD = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "p5_9_kat.json")))
+
+
+def relf(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+@pytest.fixture(scope="module")
+def cy():
+    from papers_b200 import build as b
+
+    b.build()
+    import papers_b200
+
+    return papers_b200
+
+
+def _orc_set(orc, k, P, seed, psi, reduced=False):
+    if psi == 0:
+        return orc.OracleSolver.new_with_sampler(k, P, seed, 1e-12, "sz", reduced=reduced)
+    return orc.OracleSolver.new_with_psi_sz(k, P, seed, psi, reduced=reduced)
+
+
+@pytest.mark.parametrize("psi", [0.0, 0.5, 0.1 + 0.2j])
+def test_sampler_matches_oracle(cy, orc, psi):
+    P = 20000
+    g = cy.QuinticSolver(3, P, 7, psi, fermat_variant=(psi == 0))
+    o = _orc_set(orc, 3, P, 7, psi)
+    pts, w, lo = g.get_points()
+    assert pts.shape == o.points.shape
+    # same lines, same roots; only log/cos/sin/pow last-ulp differences
+    assert np.max(np.abs(pts - o.points)) < 1e-10
+    np.testing.assert_allclose(w, o.weights, rtol=1e-9)
+    np.testing.assert_allclose(lo, o.log_omega_sq, rtol=0, atol=1e-9)
+
+
+def test_sections_bitwise_on_identical_points(cy, orc):
+    o = _orc_set(orc, 4, 3000, 3, 0.5)
+    g = cy.QuinticSolver.from_points(4, o.points, o.weights, o.log_omega_sq, psi=0.5)
+    np.testing.assert_array_equal(g.section_values, o.section_values)
+
+
+@pytest.mark.parametrize("k,psi,reduced", [(3, 0.0, False), (4, 0.5, False), (6, 0.1 + 0.2j, True)])
+def test_donaldson_fp64_parity(cy, orc, k, psi, reduced):
+    P = 20000 if k < 6 else 12000
+    o = _orc_set(orc, k, P, 11, psi, reduced)
+    g = cy.QuinticSolver.from_points(k, o.points, o.weights, o.log_omega_sq, psi=psi, reduced_basis=reduced)
+    assert g.n_basis == o.n_basis
+    for it in range(6):
+        rg = g.donaldson_step()
+        ro = o.donaldson_step()
+        assert rg == pytest.approx(ro, rel=1e-8), it
+    assert relf(g.h_block, o.h_block) <= 1e-10
+
+
+def test_sigma_fp64_parity(cy, orc):
+    o = _orc_set(orc, 3, 20000, 5, 0.5)
+    g = cy.QuinticSolver.from_points(3, o.points, o.weights, o.log_omega_sq, psi=0.5)
+    for _ in range(3):
+        o.donaldson_step()
+        g.donaldson_step()
+    so, eo = o.sigma(return_eta=True)
+    sg = g.sigma()
+    assert sg == pytest.approx(so, rel=1e-10)
+    eg = g.eta()
+    m = np.isfinite(eo)
+    assert np.array_equal(m, np.isfinite(eg))
+    np.testing.assert_allclose(eg[m], eo[m], rtol=1e-9)
+
+
+def test_fs_gram_kat_seed42(cy, orc):
+    """P5.9 protocol (p5_9_ako_apples_to_apples.rs:175-207) on the GPU, against the oracle on the same
+    points and against the reference's recorded sigma_FS / sigma_D / iteration count."""
+    rec = [r for r in GOLD["records"] if r["k"] == 3 and r["seed"] == 42][0]
+    o = orc.OracleSolver.new_with_sampler(3, rec["n_pts"], 42, 1e-12, "sz")
+    g = cy.QuinticSolver.from_points(3, o.points, o.weights, o.log_omega_sq)
+    o.orthonormalise_basis_fs_gram()
+    g.orthonormalise_basis_fs_gram()
+    sfs_o, sfs_g = o.sigma(), g.sigma()
+    assert sfs_g == pytest.approx(sfs_o, rel=1e-10)
+    assert sfs_g == pytest.approx(rec["sigma_fs_identity"], rel=1e-10)
+    it = g.donaldson_solve(50, 1e-12)
+    assert it == rec["donaldson_iters_run"]
+    sd = g.sigma()
+    assert sd == pytest.approx(rec["sigma_donaldson"], rel=1e-10)
+
+
+def test_gpu_sampler_end_to_end_kat(cy):
+    """The whole P5.9 pipeline with the GPU sampler (no oracle points)."""
+    rec = [r for r in GOLD["records"] if r["k"] == 3 and r["seed"] == 7][0]
+    g = cy.QuinticSolver.new_with_sampler(3, rec["n_pts"], 7, 1e-12, "sz")
+    g.orthonormalise_basis_fs_gram()
+    assert g.sigma() == pytest.approx(rec["sigma_fs_identity"], rel=1e-9)
+    it = g.donaldson_solve(50, 1e-12)
+    assert abs(it - rec["donaldson_iters_run"]) <= 1
+    assert g.sigma() == pytest.approx(rec["sigma_donaldson"], rel=1e-9)
+
+
+@pytest.mark.parametrize("psi", [0.0, 0.1 + 0.2j])
+def test_sigma_gradient_fp64_parity(cy, orc, psi):
+    o = _orc_set(orc, 3, 6000, 9, psi)
+    g = cy.QuinticSolver.from_points(3, o.points, o.weights, o.log_omega_sq, psi=psi)
+    for _ in range(2):
+        o.donaldson_step()
+        g.donaldson_step()
+    l2o, go, l1o = o.sigma_squared_and_gradient()
+    l2g, gg, l1g = g.sigma_squared_and_gradient()
+    assert l1g == pytest.approx(l1o, rel=1e-10)
+    assert l2g == pytest.approx(l2o, rel=1e-10)
+    assert relf(gg, go) <= 1e-9
+
+
+def test_adam_fp64_parity(cy, orc):
+    o = _orc_set(orc, 2, 4000, 13, 0.0)
+    g = cy.QuinticSolver.from_points(2, o.points, o.weights, o.log_omega_sq)
+    o.donaldson_solve(10, 1e-10)
+    g.donaldson_solve(10, 1e-10)
+    ho = o.sigma_refine_analytic(8, 1e-3)
+    hg = g.sigma_refine_analytic(8, 1e-3)
+    np.testing.assert_allclose(hg, ho, rtol=1e-9)
+    assert relf(g.h_block, o.h_block) <= 1e-9
+
+
+def test_minibatch_adam_runs_and_descends(cy):
+    g = cy.QuinticSolver.new_with_psi_sz(3, 30000, 2, 0.1 + 0.2j)
+    g.donaldson_solve(5, 1e-10)
+    s0 = g.sigma()
+    hist = g.sigma_refine_analytic(12, 2e-3, minibatch=8000, seed=5)
+    assert len(hist) == 12 and all(np.isfinite(hist))
+    assert g.sigma() < s0
+
+
+def test_error_paths(cy):
+    from papers_b200 import Cy3qError
+
+    with pytest.raises(Cy3qError) as e:
+        cy.QuinticSolver(0, 10, 1)
+    assert "ERR_ARG" in str(e.value)
+    g = cy.QuinticSolver(2, 500, 1)
+    h = g.h_block
+    h[0, 0] = np.nan
+    with pytest.raises(Cy3qError) as e:
+        g.h_block = h
+    assert "NONFINITE" in str(e.value)
+    with pytest.raises(Cy3qError) as e:
+        cy.QuinticSolver(3, 200000, 1, hbm_budget_bytes=1 << 20)
+    assert "OOM" in str(e.value)
