@@ -1,0 +1,359 @@
+"""Benchmark of the CY3 quintic metric-solver hot path on B200.
+
+Workload (one GPU): Dwork quintic sum z^5 - 5 psi prod z, psi = 0.5, degree k = 6 with the ideal-reduced
+section basis (N = 205), 500,000 line-intersection points; a step is one Donaldson balancing iteration
+(T-operator, FP64 inverse, h update).  `value` is balancing iterations per second with the points and
+section tables resident in HBM; `e2e` is the same metric through the C ABI from host buffers (points,
+weights and log|Omega|^2 uploaded from pinned memory, h_block read back); sigma evaluations per second
+and the FP64 path's iterations per second are reported beside it.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp16x3|bf16x3|fp64] [--impl reference]
+
+Under torchrun each rank runs an independent replica on its own GPU (the path has no exchange step);
+times are device times (CUDA events) and the max over ranks is reported.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "balancing iters/s & sigma evals/s at k=6, 500k pts vs FP64; p50/p99 solve lat"
+UNIT = "iters/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default=os.environ.get("CY3Q_BENCH_PRECISION", "fp16x3"))
+    ap.add_argument("--k", type=int, default=6)
+    ap.add_argument("--points", type=int, default=500_000)
+    ap.add_argument("--psi", type=float, default=0.5)
+    ap.add_argument("--seed", type=int, default=42)
+    ap.add_argument("--sigma-steps", type=int, default=5)
+    ap.add_argument("--cpu-sample", type=int, default=25_000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------------------------------------
+# clocks during the timed region
+# ------------------------------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------------------------------------------
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+    return ws, rank, local
+
+
+def dist_max(x: float, ws: int) -> float:
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def algorithmic(P, N):
+    return {
+        "F_bal": 16.0 * P * N * N,          # 8PN^2 (K = s^H h s) + 8PN^2 (T = S^H W S)
+        "F_T": 8.0 * P * N * N,
+        "F_K": 8.0 * P * N * N,
+        "F_sigma": 48.0 * P * N * N + 248.0 * P * N,
+    }
+
+
+def peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))), "measured"
+    except (OSError, ValueError):
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+def cpu_baseline(pts, w, lo, k, psi, n_full, sample, reduced=True):
+    """Balancing iteration of the FP64 oracle port on the host cores, on a bounded sample of the same
+    points; scaled linearly in points to the full workload."""
+    import oracle
+
+    oracle.set_threads(os.cpu_count() or 1)
+    n = min(sample, len(pts))
+    o = oracle.OracleSolver(pts[:n], w[:n], lo[:n], oracle.monomials(k, reduced), psi, k)
+    t0 = time.perf_counter()
+    o.donaldson_step()
+    dt = time.perf_counter() - t0
+    per_full = dt * (n_full / n)
+    return {"value": 1.0 / per_full, "unit": UNIT, "cores": oracle.threads(), "kind": "port",
+            "sample": f"1 FP64 balancing iteration on {n} of the {n_full} points (k={k}, N={o.n_basis}), "
+                      f"{dt:.2f} s, scaled linearly to {n_full} points; per-point K threaded, T-operator sum "
+                      f"serial as in the reference"}
+
+
+def run_reference(a, ws, rank):
+    if rank != 0:
+        return
+    import oracle
+
+    oracle.build()
+    # identical synthetic points to our arm (oracle sampler, same seed / psi)
+    n = a.cpu_sample
+    pts, _ = oracle.sample_sz(n, a.seed, a.psi, fermat_variant=False)
+    w = oracle.weights(pts, a.psi)
+    lo, _, _ = oracle.log_omega(pts, a.psi)
+    oracle.set_threads(os.cpu_count() or 1)
+    o = oracle.OracleSolver(pts, w, lo, oracle.monomials(a.k, True), a.psi, a.k)
+    for _ in range(max(a.warmup, 0)):
+        o.donaldson_step()
+    o.h_block = np.eye(2 * o.n_basis)
+    t0 = time.perf_counter()
+    for _ in range(a.steps):
+        o.donaldson_step()
+    dt = time.perf_counter() - t0
+    scale = a.points / n
+    v = a.steps / (dt * scale)
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": a.gpus, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": 1e3 * dt * scale / a.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"Dwork psi={a.psi} k={a.k} reduced N={o.n_basis}, {a.points} line-intersection "
+                                   f"points, one Donaldson iteration per step", "precision": "fp64",
+                       "l2": "inputs larger than L2"},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": oracle.threads(), "kind": "port",
+                             "sample": f"each step runs on {n} of the {a.points} points (oracle FP64 port of the "
+                                       f"reference Rust path), scaled linearly in points"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    a = parse()
+    ws, rank, local = dist_setup()
+    if a.impl == "reference":
+        run_reference(a, ws, rank)
+        return
+    import torch
+
+    import papers_b200
+    from papers_b200 import build as pbuild
+
+    pbuild.build()
+    torch.cuda.set_device(local)
+    dev = torch.cuda.current_device()
+    stream = torch.cuda.Stream()
+    psi = complex(a.psi)
+    # ---- sample set (untimed): GPU line-intersection sampler on this rank's GPU ----
+    s = papers_b200.QuinticSolver.new_with_psi_sz(a.k, a.points, a.seed + rank, psi, reduced_basis=True,
+                                                  precision=a.precision, with_derivs=True, device=dev)
+    s.set_stream(stream.cuda_stream)
+    P, N = s.n_points, s.n_basis
+    for _ in range(a.warmup):
+        s.donaldson_step()
+    s.h_block = np.eye(2 * N)
+
+    # ---- timed region: K balancing iterations, device-timed ----
+    clk = ClockSampler(dev)
+    clk.start()
+    time.sleep(0.3)
+    s.launch_count(reset=True)
+    s.profile(True)
+    s.profile_read(reset=True)
+    barrier(ws)
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    residuals = [s.donaldson_step() for _ in range(a.steps)]
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier(ws)
+    ms = ev0.elapsed_time(ev1)
+    clocks = clk.stop()
+    stages = s.profile_read(reset=True)
+    launches = s.launch_count(reset=True)
+    s.profile(False)
+    ms_max = dist_max(ms, ws)
+    value = ws * a.steps / (ms_max / 1e3)
+
+    h_run = s.h_block
+
+    # ---- sigma evaluations per second ----
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    sig = None
+    for _ in range(a.sigma_steps):
+        sig = s.sigma()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    sigma_ms = dist_max(ev0.elapsed_time(ev1), ws)
+    sigma_per_s = ws * a.sigma_steps / (sigma_ms / 1e3)
+
+    # ---- FP64 plain path on the same points: the 10x denominator and the accuracy reference ----
+    fp64_per_s, acc = None, None
+    if a.precision != "fp64":
+        s.set_precision("fp64")
+        s.h_block = np.eye(2 * N)
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for _ in range(a.steps):
+            s.donaldson_step()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        fp64_per_s = ws * a.steps / (dist_max(ev0.elapsed_time(ev1), ws) / 1e3)
+        h64 = s.h_block
+        sig64 = s.sigma()
+        acc = {"h_rel_frobenius": float(np.linalg.norm(h_run - h64) / np.linalg.norm(h64)),
+               "sigma_fp64": sig64, "sigma_rel_err": abs(sig / sig64 - 1.0) if sig else None,
+               "iterations": a.steps}
+        s.set_precision(a.precision)
+        s.h_block = h_run
+    else:
+        fp64_per_s = value
+
+    # ---- e2e through the C ABI from pinned host buffers ----
+    pts, w, lo = s.get_points()
+    hp = torch.from_numpy(pts).pin_memory()
+    hw = torch.from_numpy(w).pin_memory()
+    hl = torch.from_numpy(lo).pin_memory()
+    e = papers_b200.QuinticSolver(a.k, 0, 0, psi, fermat_variant=False, reduced_basis=True, precision=a.precision,
+                                  with_derivs=False, device=dev, sample=False)
+    e.set_stream(stream.cuda_stream)
+    h_out = np.empty((2 * N, 2 * N))
+    torch.cuda.synchronize()
+    barrier(ws)
+    t0 = time.perf_counter()
+    ev0.record(stream)
+    e.set_points(hp.numpy(), hw.numpy(), hl.numpy())
+    for _ in range(a.steps):
+        e.donaldson_step()
+    h_out[:] = e.h_block
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = dist_max(ev0.elapsed_time(ev1), ws)
+    e2e_wall = dist_max(time.perf_counter() - t0, ws)
+    e.close()
+    h2d = (pts.nbytes + w.nbytes + lo.nbytes) / a.steps
+    d2h = (h_out.nbytes + 8 * a.steps) / a.steps
+    e2e_value = ws * a.steps / (e2e_ms / 1e3)
+
+    # ---- roofline of the dominant stage ----
+    pk, src = peaks()
+    alg = algorithmic(P, N)
+    dom = max(stages.items(), key=lambda kv: kv[1][0]) if stages else ("toperator", (ms, a.steps))
+    stage_flops = {"toperator": alg["F_T"], "bergman": alg["F_K"]}
+    if a.precision == "fp64":
+        peak_tf, peak_note = 37.0, "nominal FP64 peak (no measured FP64 figure in MEASURED_PEAKS.json)"
+    else:
+        peak_tf, peak_note = pk["bf16_tflops_sustained"], f"{src} bf16 dense, sustained"
+    dname, (dms, dcalls) = dom
+    avg_ms = dms / max(dcalls, 1)
+    achieved = stage_flops.get(dname, alg["F_T"]) / (avg_ms / 1e3) / 1e12
+    roof = {"bound": "tensor", "achieved": achieved, "peak": peak_tf, "unit": "TFLOP/s", "frac": achieved / peak_tf,
+            "traffic": None, "kernel_stage": dname, "avg_launch_ms": avg_ms, "peak_source": peak_note,
+            "stage_ms_per_step": {k: v[0] / max(v[1], 1) for k, v in stages.items()}}
+
+    cpu = None
+    if rank == 0 and ws == 1 and not a.no_cpu_baseline:
+        cpu = cpu_baseline(pts, w, lo, a.k, psi, P, a.cpu_sample)
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": a.steps, "warmup": a.warmup,
+                "ms_per_step": ms_max / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64" if a.precision == "fp64" else a.precision, "data": "synthetic",
+                "config": {"workload": f"Dwork psi={a.psi} k={a.k} reduced N={N}, {P} line-intersection points "
+                                       f"(seeded LCG, GPU sampler), one Donaldson balancing iteration per step",
+                           "precision": a.precision, "parallelism": f"replicas x{ws}",
+                           "l2": "inputs larger than L2 (section table %.2f GB)" % (P * 6 * (2 * N + 30) * 8 / 1e9)},
+                "sigma_evals_per_s": sigma_per_s, "sigma": sig, "fp64_iters_per_s": fp64_per_s,
+                "accuracy_vs_fp64": acc,
+                "speedup_vs_fp64": (value / fp64_per_s) if fp64_per_s else None,
+                "residual_last": residuals[-1],
+                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                        "wall_s": e2e_wall},
+                "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu, "clocks": clocks}
+        print(json.dumps(line), flush=True)
+    s.close()
+    if ws > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

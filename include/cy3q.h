@@ -180,6 +180,25 @@ cy3q_status cy3q_server_stats_get(cy3q_server* srv, cy3q_server_stats* out);
 /* h of a completed request, [2N x 2N] in the reference packing. */
 cy3q_status cy3q_result_h(cy3q_server* srv, uint64_t ticket, double* h_block);
 
+/* ---- per-stage device timing (tracing; the reference's nearest analogue is
+        AdamGradientKernel::compute_sigma_grad_h_only_profiled, gpu_adam.rs:1626-1767) ---- */
+typedef enum {
+  CY3Q_STAGE_BERGMAN = 0,     /* K_p = s^H h s: GEMM + row dot */
+  CY3Q_STAGE_TOPERATOR = 1,   /* T = S^H diag(w/K) S contraction over the points */
+  CY3Q_STAGE_TREDUCE = 2,     /* split reduction, /sum w, trace renormalisation */
+  CY3Q_STAGE_INVERSE = 3,     /* FP64 Cholesky + inverse of T */
+  CY3Q_STAGE_PACK = 4,        /* h_block packing + residual */
+  CY3Q_STAGE_SIGMA_GEMM = 5,  /* h applied to s and d s */
+  CY3Q_STAGE_SIGMA_POINT = 6, /* per-point metric algebra + reductions */
+  CY3Q_STAGE_GRAD = 7,        /* gradient rows + contractions + assembly */
+  CY3Q_STAGE_OPERANDS = 8,    /* split-precision operand preparation */
+  CY3Q_STAGE_COUNT = 9
+} cy3q_stage;
+/* Records CUDA events around each stage (no extra synchronisation while enabled). */
+cy3q_status cy3q_profile_enable(cy3q_solver* s, int32_t on);
+/* Waits for the handle's stream and returns the accumulated device time and call count of a stage. */
+cy3q_status cy3q_profile_read(cy3q_solver* s, int32_t stage, double* total_ms, uint64_t* calls, int32_t reset);
+
 /* ---- build / device information ---- */
 const char* cy3q_version(void);
 /* Number of this library's kernels launched by the handle since the last reset. */

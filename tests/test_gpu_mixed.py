@@ -1,0 +1,67 @@
+"""Split-precision tensor-core balancing (tcgen05 kind::f16, FP32 TMEM accumulation flushed to FP64)
+against the FP64 path on identical points.
+
+Tolerances (north star: sigma within 1e-6 relative of the FP64 oracle for the mixed-precision loop):
+  * fp16x3 (the default split): h after the iterations within 2e-6 relative Frobenius of the FP64 path,
+    sigma within 1e-6
+  * bf16x3: h within 2e-5, sigma within 1e-5 -- the bf16 hi/lo split carries 16 significant bits, which
+    bounds its accuracy at k = 6 to a few 1e-6; it is offered for range, not for the 1e-6 target
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+TOL_H = {"fp16x3": 2e-6, "bf16x3": 2e-5}
+TOL_SIGMA = {"fp16x3": 1e-6, "bf16x3": 1e-5}
+
+
+def relf(a, b):
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+@pytest.fixture(scope="module")
+def cy():
+    from papers_b200 import build as b
+
+    b.build()
+    import papers_b200
+
+    return papers_b200
+
+
+@pytest.mark.parametrize("prec", ["fp16x3", "bf16x3"])
+@pytest.mark.parametrize("k,psi,reduced,P", [(3, 0.0, False, 20000), (4, 0.5, False, 30000),
+                                             (6, 0.1 + 0.2j, True, 40000)])
+def test_mixed_balancing_matches_fp64(cy, orc, prec, k, psi, reduced, P):
+    if psi == 0:
+        o = orc.OracleSolver.new_with_sampler(k, P, 21, 1e-12, "sz", reduced=reduced)
+    else:
+        o = orc.OracleSolver.new_with_psi_sz(k, P, 21, psi, reduced=reduced)
+    f = cy.QuinticSolver.from_points(k, o.points, o.weights, o.log_omega_sq, psi=psi, reduced_basis=reduced)
+    m = cy.QuinticSolver.from_points(k, o.points, o.weights, o.log_omega_sq, psi=psi, reduced_basis=reduced,
+                                     precision=prec)
+    # one step from h = I isolates the two contractions
+    rf, rm = f.donaldson_step(), m.donaldson_step()
+    assert rm == pytest.approx(rf, rel=1e-4)
+    assert relf(m.h_block, f.h_block) < TOL_H[prec]
+    for _ in range(7):
+        f.donaldson_step()
+        m.donaldson_step()
+    assert relf(m.h_block, f.h_block) < TOL_H[prec]
+    sf, sm = f.sigma(), m.sigma()
+    assert sm == pytest.approx(sf, rel=TOL_SIGMA[prec])
+
+
+def test_mixed_fs_gram_kat(cy, orc):
+    """P5.9 protocol with the split-precision balancing loop: sigma_D within 1e-6 of the reference record."""
+    import json
+    import os
+
+    gold = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "p5_9_kat.json")))
+    rec = [r for r in gold["records"] if r["k"] == 3 and r["seed"] == 42][0]
+    o = orc.OracleSolver.new_with_sampler(3, rec["n_pts"], 42, 1e-12, "sz")
+    m = cy.QuinticSolver.from_points(3, o.points, o.weights, o.log_omega_sq, precision="fp16x3")
+    m.orthonormalise_basis_fs_gram()
+    m.donaldson_solve(rec["donaldson_iters_run"], 0.0)
+    assert m.sigma() == pytest.approx(rec["sigma_donaldson"], rel=1e-6)
