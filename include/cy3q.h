@@ -199,6 +199,23 @@ cy3q_status cy3q_profile_enable(cy3q_solver* s, int32_t on);
 /* Waits for the handle's stream and returns the accumulated device time and call count of a stage. */
 cy3q_status cy3q_profile_read(cy3q_solver* s, int32_t stage, double* total_ms, uint64_t* calls, int32_t reset);
 
+/* ---- sigma without device allocation (this entry point has no counterpart in the reference) ----
+   For callers that must not have the library allocate device memory (a process that reserved its HBM
+   in one arena at start-up, a fixed per-process memory budget on a shared GPU, or a loop in which a
+   cudaMalloc / cudaFree -- which may synchronise the whole device -- is not acceptable).  Computes the
+   same sigma_L1 and per-point eta as cy3q_sigma (monomial basis, no FS-Gram transform) for the
+   h_block given in device memory; all inputs and the eta output are caller-owned DEVICE buffers.
+   Intermediates live in one fixed device array inside the library (about 7 MiB, held on every GPU
+   that loads the library until exit); its address is looked up by the first call on each device, so
+   make that first call before any stream capture.  Calls share that array: calls that overlap on the
+   GPU race.  Rejects bases of more than CY3Q_NOALLOC_MAX_BASIS sections with CY3Q_ERR_SHAPE.
+   cuda_stream may be NULL (legacy default stream).  The call waits for its stream before returning. */
+#define CY3Q_NOALLOC_MAX_BASIS 224
+cy3q_status cy3q_sigma_noalloc(int32_t device, uint32_t k, int32_t reduced_basis, double psi_re, double psi_im,
+                               const double* d_points, const double* d_weights, const double* d_log_omega,
+                               uint64_t n_points, const double* d_h_block, double* d_eta, double* sigma_l1,
+                               void* cuda_stream);
+
 /* ---- build / device information ---- */
 const char* cy3q_version(void);
 /* Number of this library's kernels launched by the handle since the last reset. */
