@@ -295,14 +295,19 @@ def main():
                                   with_derivs=False, device=dev, sample=False)
     e.set_stream(stream.cuda_stream)
     h_out = np.empty((2 * N, 2 * N))
+
+    def e2e_run():
+        e.set_points(hp.numpy(), hw.numpy(), hl.numpy())
+        for _ in range(a.steps):
+            e.donaldson_step()
+        h_out[:] = e.h_block
+
+    e2e_run()  # warm: device buffers of the handle are allocated once and reused
     torch.cuda.synchronize()
     barrier(ws)
     t0 = time.perf_counter()
     ev0.record(stream)
-    e.set_points(hp.numpy(), hw.numpy(), hl.numpy())
-    for _ in range(a.steps):
-        e.donaldson_step()
-    h_out[:] = e.h_block
+    e2e_run()
     ev1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = dist_max(ev0.elapsed_time(ev1), ws)
@@ -315,17 +320,27 @@ def main():
     # ---- roofline of the dominant stage ----
     pk, src = peaks()
     alg = algorithmic(P, N)
-    dom = max(stages.items(), key=lambda kv: kv[1][0]) if stages else ("toperator", (ms, a.steps))
+    # DRAM bytes per point of the tensor-core kernels, from the ncu capture of the same kernels on a
+    # 100,096-point case (profiles/umma_*_k6.md), scaled linearly in points
+    traffic_per_point = {"bergman": (180.232192e6 + 6.467072e6) / 100096,
+                         "toperator": (179.593984e6 + 4.617472e6) / 100096}
     stage_flops = {"toperator": alg["F_T"], "bergman": alg["F_K"]}
+    cand = {k: v for k, v in stages.items() if k in stage_flops}
+    dname, (dms, dcalls) = max(cand.items(), key=lambda kv: kv[1][0]) if cand else ("toperator", (ms, a.steps))
     if a.precision == "fp64":
-        peak_tf, peak_note = 37.0, "nominal FP64 peak (no measured FP64 figure in MEASURED_PEAKS.json)"
+        peak_tf, peak_note = 37.0, "nominal FP64 peak (MEASURED_PEAKS.json has no FP64 figure)"
+        traffic = None
     else:
-        peak_tf, peak_note = pk["bf16_tflops_sustained"], f"{src} bf16 dense, sustained"
-    dname, (dms, dcalls) = dom
+        peak_tf, peak_note = pk["bf16_tflops"], f"{src} bf16 dense, burst (each kernel runs < 1 ms)"
+        traffic = traffic_per_point[dname] * P
     avg_ms = dms / max(dcalls, 1)
-    achieved = stage_flops.get(dname, alg["F_T"]) / (avg_ms / 1e3) / 1e12
+    achieved = stage_flops[dname] / (avg_ms / 1e3) / 1e12
     roof = {"bound": "tensor", "achieved": achieved, "peak": peak_tf, "unit": "TFLOP/s", "frac": achieved / peak_tf,
-            "traffic": None, "kernel_stage": dname, "avg_launch_ms": avg_ms, "peak_source": peak_note,
+            "traffic": traffic, "kernel_stage": dname, "avg_launch_ms": avg_ms, "peak_source": peak_note,
+            "algorithmic_flops_per_launch": stage_flops[dname],
+            "note": "achieved counts algorithmic flops (8PN^2 per GEMM); the split-precision tensor pipe executes "
+                    "3 products per flop on padded tiles, so the ceiling of frac is about 1/3",
+            "traffic_note": "DRAM bytes per launch scaled from the 100k-point ncu capture",
             "stage_ms_per_step": {k: v[0] / max(v[1], 1) for k, v in stages.items()}}
 
     cpu = None
