@@ -45,6 +45,9 @@ def parse():
     ap.add_argument("--sigma-steps", type=int, default=5)
     ap.add_argument("--cpu-sample", type=int, default=25_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--serving-requests", type=int, default=256, help="0 skips the serving stream")
+    ap.add_argument("--serving-rate", type=float, default=50.0)
+    ap.add_argument("--serving-active", type=int, default=8)
     return ap.parse_args()
 
 
@@ -166,6 +169,64 @@ def cpu_baseline(pts, w, lo, k, psi, n_full, sample, reduced=True):
             "sample": f"1 FP64 balancing iteration on {n} of the {n_full} points (k={k}, N={o.n_basis}), "
                       f"{dt:.2f} s, scaled linearly to {n_full} points; per-point K threaded, T-operator sum "
                       f"serial as in the reference"}
+
+
+N_REDUCED = {2: 15, 3: 35, 4: 70, 5: 125, 6: 205, 7: 315, 8: 460}
+
+
+def serving_stream(a, dev):
+    """Config 5: Poisson arrivals (mean rate a.serving_rate / s), psi uniform in the unit disk, k uniform in
+    {2..8}, P = min(10 N^2, 2,000,000), 10 balancing iterations each, split precision; continuous batching
+    by the library's server.  The one-at-a-time FP64 reference times one FP64 solve per k and weights it by
+    the request mix."""
+    from papers_b200 import cy3q
+
+    rng = np.random.default_rng(2026)
+    reqs = []
+    t = 0.0
+    for i in range(a.serving_requests):
+        t += rng.exponential(1.0 / a.serving_rate)
+        k = int(rng.integers(2, 9))
+        u, v = rng.random(), rng.random()
+        psi = np.sqrt(u) * np.exp(2j * np.pi * v)
+        reqs.append((t, dict(k=k, n_points=min(10 * N_REDUCED[k] ** 2, 2_000_000), seed=1000 + i, psi=psi,
+                             iterations=10, precision=a.precision)))
+    srv = cy3q.Server(dev, 0, a.serving_active)
+    t0 = time.perf_counter()
+    tickets = []
+    for at, r in reqs:
+        d = at - (time.perf_counter() - t0)
+        if d > 0:
+            time.sleep(d)
+        tickets.append(srv.submit(**r))
+    failed = 0
+    for tk in tickets:
+        if srv.wait(tk, 600000).status != 0:
+            failed += 1
+    wall = time.perf_counter() - t0
+    st = srv.stats()
+    srv.close()
+    # one-at-a-time FP64 reference on the same GPU
+    per_k = {}
+    for k in sorted({r["k"] for _, r in reqs}):
+        n = min(10 * N_REDUCED[k] ** 2, 2_000_000)
+        s = cy3q.QuinticSolver.new_with_psi_sz(k, n, 7, 0.5, reduced_basis=True, precision="fp64",
+                                               with_derivs=False, device=dev)
+        import torch
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        for _ in range(10):
+            s.donaldson_step()
+        per_k[k] = time.perf_counter() - t1
+        s.close()
+    fp64_total = sum(per_k[r["k"]] for _, r in reqs)
+    iters = sum(r["iterations"] for _, r in reqs)
+    return {"requests": len(reqs), "failed": failed, "arrival_rate_per_s": a.serving_rate,
+            "max_active": a.serving_active, "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
+            "iters_per_s": st["iters_per_s"], "wall_s": wall, "hbm_peak_bytes": st["hbm_peak"],
+            "fp64_one_at_a_time_iters_per_s": iters / fp64_total,
+            "fp64_one_at_a_time_s_per_solve_by_k": {str(k): v for k, v in per_k.items()},
+            "precision": a.precision}
 
 
 def run_reference(a, ws, rank):
@@ -343,6 +404,11 @@ def main():
             "traffic_note": "DRAM bytes per launch scaled from the 100k-point ncu capture",
             "stage_ms_per_step": {k: v[0] / max(v[1], 1) for k, v in stages.items()}}
 
+    serving = None
+    if a.serving_requests > 0:
+        barrier(ws)
+        serving = serving_stream(a, dev)
+
     cpu = None
     if rank == 0 and ws == 1 and not a.no_cpu_baseline:
         cpu = cpu_baseline(pts, w, lo, a.k, psi, P, a.cpu_sample)
@@ -361,7 +427,8 @@ def main():
                 "residual_last": residuals[-1],
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                         "wall_s": e2e_wall},
-                "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu, "clocks": clocks}
+                "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu, "clocks": clocks,
+                "serving": serving}
         print(json.dumps(line), flush=True)
     s.close()
     if ws > 1:

@@ -53,6 +53,21 @@ def test_mixed_balancing_matches_fp64(cy, orc, prec, k, psi, reduced, P):
     assert sm == pytest.approx(sf, rel=TOL_SIGMA[prec])
 
 
+@pytest.mark.parametrize("k,reduced,P", [(2, False, 3000), (7, True, 30000), (8, True, 30000)])
+def test_mixed_small_and_large_bases(cy, orc, k, reduced, P):
+    """Operand shapes from one 64-wide k-stage (k = 2) to 15 (k = 8, N = 460, 36 T tiles)."""
+    psi = 0.2 - 0.1j
+    o = orc.OracleSolver.new_with_psi_sz(k, P, 5, psi, reduced=reduced)
+    f = cy.QuinticSolver.from_points(k, o.points, o.weights, o.log_omega_sq, psi=psi, reduced_basis=reduced,
+                                     with_derivs=False)
+    m = cy.QuinticSolver.from_points(k, o.points, o.weights, o.log_omega_sq, psi=psi, reduced_basis=reduced,
+                                     with_derivs=False, precision="fp16x3")
+    for _ in range(2):
+        f.donaldson_step()
+        m.donaldson_step()
+    assert relf(m.h_block, f.h_block) < 1e-5
+
+
 def test_mixed_fs_gram_kat(cy, orc):
     """P5.9 protocol with the split-precision balancing loop: sigma_D within 1e-6 of the reference record."""
     import json
