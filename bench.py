@@ -48,6 +48,7 @@ def parse():
     ap.add_argument("--serving-requests", type=int, default=256, help="0 skips the serving stream")
     ap.add_argument("--serving-rate", type=float, default=50.0)
     ap.add_argument("--serving-active", type=int, default=8)
+    ap.add_argument("--galerkin-points", type=int, default=1_000_000, help="0 skips the Laplacian / Yukawa run")
     return ap.parse_args()
 
 
@@ -229,6 +230,57 @@ def serving_stream(a, dev):
             "precision": a.precision}
 
 
+def galerkin_run(a, dev, stream, h_block):
+    """Config 4: Laplacian spectrum on the balanced k=6 metric of the timed run (its h), assembled over
+    fresh line-intersection points in split precision and in FP64; 40 lowest eigenvalues; 3x3x3 Yukawa
+    overlap from seeded CN(0,1) coefficients over the same points."""
+    import torch
+
+    import papers_b200
+
+    g = papers_b200.QuinticSolver.new_with_psi_sz(a.k, a.galerkin_points, a.seed + 1000, complex(a.psi),
+                                                  reduced_basis=True, precision=a.precision, with_derivs=True,
+                                                  device=dev)
+    g.set_stream(stream.cuda_stream)
+    g.h_block = h_block
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed(fn):
+        fn()  # warm: scratch pool, cuSOLVER workspace
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        out = fn()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        return out, ev0.elapsed_time(ev1)
+
+    g.profile(True)
+    g.profile_read(reset=True)
+    ev, ms_split = timed(lambda: g.laplacian(40, 2, reg=1e-12))
+    st_split = {k: v[0] / max(v[1], 1) for k, v in g.profile_read(reset=True).items()}
+    g.set_precision("fp64")
+    ev64, ms_64 = timed(lambda: g.laplacian(40, 2, reg=1e-12))
+    st_64 = {k: v[0] / max(v[1], 1) for k, v in g.profile_read(reset=True).items()}
+    g.set_precision(a.precision)
+    rng = np.random.default_rng(a.seed)
+    coeffs = (rng.standard_normal((3, 225)) + 1j * rng.standard_normal((3, 225))) / np.sqrt(2.0)
+    y, ms_y = timed(lambda: g.yukawa(coeffs))
+    g.profile(False)
+    P = g.n_points
+    g.close()
+    scale = np.maximum(np.abs(ev64), 1.0)
+    scale[0] = 1.0
+    nf = 225
+    flops = 2.0 * P * (2 * nf) ** 2 * 4  # real Gram flops: mass (P rows) + stiffness (3P rows)
+    return {"points": P, "n_functions": nf, "precision": a.precision, "ms": ms_split, "fp64_ms": ms_64,
+            "speedup_vs_fp64": ms_64 / ms_split, "eig_max_rel_err_vs_fp64": float(np.max(np.abs(ev - ev64) / scale)),
+            "eigs_lowest": [float(x) for x in ev[:6]], "eig_40": float(ev[-1]),
+            "stage_ms": st_split, "fp64_stage_ms": st_64,
+            "gram_tflops_algorithmic": flops / (st_split.get("galerkin_gram", float("nan")) / 1e3) / 1e12,
+            "yukawa_ms": ms_y, "yukawa_abs_max": float(np.abs(y).max()), "yukawa_000": [y[0, 0, 0].real, y[0, 0, 0].imag],
+            "coefficients": "CN(0,1), numpy default_rng(seed), 3 x 225"}
+
+
 def run_reference(a, ws, rank):
     if rank != 0:
         return
@@ -404,6 +456,11 @@ def main():
             "traffic_note": "DRAM bytes per launch scaled from the 100k-point ncu capture",
             "stage_ms_per_step": {k: v[0] / max(v[1], 1) for k, v in stages.items()}}
 
+    galerkin = None
+    if a.galerkin_points > 0:
+        barrier(ws)
+        galerkin = galerkin_run(a, dev, stream, h_run)
+
     serving = None
     if a.serving_requests > 0:
         barrier(ws)
@@ -428,7 +485,7 @@ def main():
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                         "wall_s": e2e_wall},
                 "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu, "clocks": clocks,
-                "serving": serving}
+                "laplacian": galerkin, "serving": serving}
         print(json.dumps(line), flush=True)
     s.close()
     if ws > 1:

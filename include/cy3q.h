@@ -129,18 +129,31 @@ cy3q_status cy3q_sigma_grad(cy3q_solver* s, double* sigma_l2sq, double* grad, do
 cy3q_status cy3q_adam_refine(cy3q_solver* s, int32_t steps, double lr, uint64_t minibatch, uint64_t seed,
                              double* history, int32_t* steps_done);
 
-/* ---- Laplacian Galerkin spectrum + Yukawa overlap (templates: route34/metric_laplacian.rs:296-710,
-        route34/yukawa_overlap_real.rs:372) ---- */
+/* ---- Laplacian Galerkin spectrum + Yukawa overlap (templates: route34/metric_laplacian.rs:296-531,
+        route34/yukawa_overlap_real.rs:298-372; the reference has no quintic version) ----
+   Test functions f_ab = s_a conj(s_b) / (z^H z)^d, s the degree-d monomials (d = 1: 25 functions,
+   d = 2: 225), indexed al = a * n_d + b in the monomial order of the basis.  Integration measure
+   c_p = w_p eta_p (the volume form of the metric of the current h); points the sigma functional skips
+   are left out.  Assembly uses the handle's precision: FP64, or the tensor cores with a 16-bit hi/lo
+   split (four products); the per-point metric is always FP64. */
 typedef struct {
-  uint32_t test_degree;      /* degree of the sections s in the (d,d) test functions f = s_a conj(s_b) / K^d */
-  uint32_t n_eigs;           /* lowest eigenvalues returned */
-  double reg;                /* relative Tikhonov regularisation of the mass matrix */
+  uint32_t test_degree;      /* d in f_ab above: 1 or 2 */
+  uint32_t n_eigs;           /* lowest eigenvalues returned (by magnitude), 1 .. n_functions */
+  double reg;                /* mass-matrix shift reg * |M|_F (metric_laplacian.rs:547-553 uses 1e-10) */
 } cy3q_laplacian_config;
-/* Assembles mass and stiffness matrices over the solver's points with the current balanced h and
-   returns the lowest n_eigs eigenvalues of K v = lambda M v (FP64 eigensolve).  eigs [n_eigs]. */
+/* Lowest n_eigs magnitudes of the eigenvalues of K v = lambda (M + reg |M|_F I) v, ascending (FP64
+   generalised Hermitian eigensolve on the device; metric_laplacian.rs:296-392).  eigs [n_eigs]. */
 cy3q_status cy3q_laplacian(cy3q_solver* s, const cy3q_laplacian_config* cfg, double* eigs);
-/* Y_ijk = sum_p w_p psi_i psi_j psi_k conj(Omega_p) / sum_p w_p with psi_i = sum_alpha c_{i,alpha} f_alpha
-   (n_modes x M complex coefficients, interleaved), y [n_modes^3 x 2]. */
+/* The assembled mass and stiffness matrices (no reference counterpart; exposes build_mass_matrix /
+   build_stiffness_matrix, metric_laplacian.rs:424-531): M = sum c conj(f_al) f_be / sum c,
+   K = sum c g^{ab~} conj(d_b f_al) d_a f_be / sum c, row-major n x n complex (interleaved re, im).
+   *n_functions receives n; with mass == stiffness == NULL only n is returned. */
+cy3q_status cy3q_laplacian_matrices(cy3q_solver* s, const cy3q_laplacian_config* cfg, double* mass,
+                                    double* stiffness, uint32_t* n_functions);
+/* Y_ijk = sum_p w_p psi_i psi_j psi_k conj(Omega_p) / sum_p w_p (yukawa_overlap_real.rs:298-349) with
+   psi_i = sum_al c_{i,al} f_al over the sampler weights w_p; Omega_p = z_chart / (df/dz_elim)
+   (quintic.rs:4894-4909).  coeffs [n_modes][n_functions] complex interleaved, n_modes 1..4;
+   y [n_modes^3] complex interleaved, index (i n_modes + j) n_modes + k. */
 cy3q_status cy3q_yukawa(cy3q_solver* s, const cy3q_laplacian_config* cfg, const double* coeffs, uint32_t n_modes,
                         double* y);
 
@@ -192,7 +205,11 @@ typedef enum {
   CY3Q_STAGE_SIGMA_POINT = 6, /* per-point metric algebra + reductions */
   CY3Q_STAGE_GRAD = 7,        /* gradient rows + contractions + assembly */
   CY3Q_STAGE_OPERANDS = 8,    /* split-precision operand preparation */
-  CY3Q_STAGE_COUNT = 9
+  CY3Q_STAGE_GALERKIN_ROWS = 9,   /* Laplacian test-function rows (mass + stiffness) */
+  CY3Q_STAGE_GALERKIN_GRAM = 10,  /* mass / stiffness Gram contractions */
+  CY3Q_STAGE_GALERKIN_EIGEN = 11, /* FP64 generalised Hermitian eigensolve */
+  CY3Q_STAGE_YUKAWA = 12,         /* Yukawa overlap */
+  CY3Q_STAGE_COUNT = 13
 } cy3q_stage;
 /* Records CUDA events around each stage (no extra synchronisation while enabled). */
 cy3q_status cy3q_profile_enable(cy3q_solver* s, int32_t on);

@@ -77,6 +77,12 @@ def lib():
     L.orc_sigma_grad.restype = C.c_int
     L.orc_adam_refine.argtypes = [_dp, _dp, _dp, _dp, _dp, sz, C.c_int, d, d, _dp, C.c_int, d, d, d, d, _dp]
     L.orc_adam_refine.restype = C.c_int
+    L.orc_laplacian_rows.argtypes = [_dp, _dp, _dp, _dp, _dp, sz, C.c_int, d, d, _dp, C.c_int, _dp, _dp, _dp]
+    L.orc_laplacian_rows.restype = C.c_int
+    L.orc_laplacian_gram.argtypes = [_dp, _dp, _dp, sz, C.c_int, _dp, _dp]
+    L.orc_laplacian_gram.restype = d
+    L.orc_yukawa.argtypes = [_dp, _dp, sz, d, d, C.c_int, _dp, C.c_int, _dp]
+    L.orc_yukawa.restype = C.c_int
     _lib = L
     return L
 
@@ -304,6 +310,39 @@ class OracleSolver:
                              self.h_block.reshape(-1), C.byref(l2), g, C.byref(l1))
         return l2.value, g, l1.value
 
+    def laplacian_rows(self, test_degree: int = 2):
+        """Per-point Galerkin rows at the current h: f [P][nf], e [P][3][nf] (complex) and c_p = w_p eta_p."""
+        nd = len(monomials(test_degree))
+        nf = nd * nd
+        P = self.n_points
+        F = np.empty((P, nf), np.complex128)
+        E = np.empty((P, 3, nf), np.complex128)
+        c = np.empty(P, np.float64)
+        got = lib().orc_laplacian_rows(self.section_values.reshape(-1), self.section_derivs.reshape(-1),
+                                       self.points.reshape(-1), self.weights, self.log_omega_sq, P, self.n_basis,
+                                       self.psi.real, self.psi.imag, self.h_block.reshape(-1), test_degree,
+                                       F.view(np.float64).reshape(-1), E.view(np.float64).reshape(-1), c)
+        if got != nf:
+            raise ValueError("unsupported test degree")
+        return F, E, c
+
+    def laplacian_matrices(self, test_degree: int = 2):
+        """Galerkin mass and stiffness matrices (complex nf x nf, normalised by sum c) at the current h."""
+        return laplacian_gram(*self.laplacian_rows(test_degree))
+
+    def laplacian_eigs(self, n_eigs: int = 40, test_degree: int = 2, reg: float = 1e-12):
+        return laplacian_eigs(*self.laplacian_matrices(test_degree), n_eigs=n_eigs, reg=reg)
+
+    def yukawa(self, coeffs: np.ndarray, test_degree: int = 2) -> np.ndarray:
+        c = np.ascontiguousarray(coeffs, dtype=np.complex128)
+        nm = c.shape[0]
+        y = np.empty(nm ** 3, np.complex128)
+        got = lib().orc_yukawa(self.points.reshape(-1), self.weights, self.n_points, self.psi.real, self.psi.imag,
+                               test_degree, c.view(np.float64).reshape(-1), nm, y.view(np.float64).reshape(-1))
+        if got < 0:
+            raise ValueError("unsupported test degree or mode count")
+        return y.reshape(nm, nm, nm)
+
     def sigma_refine_analytic(self, n_iter: int, lr: float, beta1=0.9, beta2=0.999, eps=1e-8):
         """QuinticSolver::sigma_refine_analytic (quintic.rs:453)."""
         hist = np.empty(max(n_iter, 1))
@@ -312,3 +351,27 @@ class OracleSolver:
                                      self.n_basis, self.psi.real, self.psi.imag, self.h_block.reshape(-1), n_iter, lr,
                                      beta1, beta2, eps, hist)
         return list(hist[:done])
+
+
+def laplacian_gram(F: np.ndarray, E: np.ndarray, c: np.ndarray):
+    """M = sum c conj(f) f^T / sum c and K = sum c e^H e / sum c, accumulated point by point in FP64."""
+    F = np.ascontiguousarray(F, np.complex128)
+    E = np.ascontiguousarray(E, np.complex128)
+    c = np.ascontiguousarray(c, np.float64)
+    P, nf = F.shape
+    M = np.empty((nf, nf), np.complex128)
+    K = np.empty((nf, nf), np.complex128)
+    lib().orc_laplacian_gram(F.view(np.float64).reshape(-1), E.view(np.float64).reshape(-1), c, P, nf,
+                             M.view(np.float64).reshape(-1), K.view(np.float64).reshape(-1))
+    return M, K
+
+
+def laplacian_eigs(M: np.ndarray, K: np.ndarray, n_eigs: int = 40, reg: float = 1e-12) -> np.ndarray:
+    """Lowest n_eigs of K v = lambda (M + reg |M|_F I) v by magnitude (metric_laplacian.rs:350-392:
+    Frobenius-scaled Tikhonov shift of the mass matrix, eigenvalues sorted by |lambda|)."""
+    import scipy.linalg
+
+    n = M.shape[0]
+    Mr = M + reg * np.linalg.norm(M) * np.eye(n)
+    ev = scipy.linalg.eigh(K, Mr, eigvals_only=True)
+    return np.sort(np.abs(ev))[:n_eigs]

@@ -1373,3 +1373,240 @@ int orc_adam_refine(const double* s, const double* ds, const double* pts, const 
 }
 
 }  // extern "C"
+
+// =======================================================================================
+// Laplacian Galerkin assembly and Yukawa overlap.  The reference has no quintic version; its templates
+// are route34/metric_laplacian.rs:424-531 (mass / stiffness sums over the sample, normalised by the
+// weight sum) and route34/yukawa_overlap_real.rs:298-349 (Y_ijk = sum w psi_i psi_j psi_k conj(Omega)).
+// Test functions f_ab = s_a conj(s_b) / (z^H z)^d with s the degree-d monomials (d = 1, 2): homogeneous
+// of degree zero, so they are functions on the quintic.  With c_p = w_p eta_p (the volume form of the
+// metric g of h: det g_tan = eta |Omega|^2) and e = L^{-1} D f (g_tan = L L^H, D_t f = sum_i T_t[i] d_i f
+// along the affine-chart frame T):
+//   M_{al,be} = sum_p c_p conj(f_al) f_be / sum c,   K_{al,be} = sum_p c_p e_al^H e_be / sum c
+// i.e. K = int g^{ab~} conj(d_b f_al) d_a f_be dvol_g, the Dirichlet form of the Laplacian of g.
+// =======================================================================================
+namespace {
+
+// degree-d monomial values and first derivatives at z: sv[nd], dsv[5][nd]
+void small_basis(const double* z, const uint32_t* mono, int nd, C* sv, C* dsv) {
+  for (int a = 0; a < nd; ++a) {
+    const uint32_t* m = mono + 5 * a;
+    C v = {1.0, 0.0};
+    for (int j = 0; j < 5; ++j)
+      for (uint32_t e = 0; e < m[j]; ++e) v = cmul(v, C{z[2 * j], z[2 * j + 1]});
+    sv[a] = v;
+    for (int i = 0; i < 5; ++i) {
+      C dv = {0.0, 0.0};
+      if (m[i] > 0) {
+        dv = {(double)m[i], 0.0};
+        for (int j = 0; j < 5; ++j) {
+          uint32_t ex = m[j] - (j == i ? 1u : 0u);
+          for (uint32_t e = 0; e < ex; ++e) dv = cmul(dv, C{z[2 * j], z[2 * j + 1]});
+        }
+      }
+      dsv[i * nd + a] = dv;
+    }
+  }
+}
+
+// Rows of one point: f[nf], e[3][nf]; returns c_p = w_p eta_p (0 for a point the sigma functional skips).
+double lap_point(const double* s, const double* ds, const double* h, int N, const double* z, double w, double lo,
+                 double psr, double psi, const uint32_t* mono, int nd, int d, C* f, C* e) {
+  const int nf = nd * nd;
+  for (int q = 0; q < nf; ++q) f[q] = {0, 0};
+  for (int q = 0; q < 3 * nf; ++q) e[q] = {0, 0};
+  if (!std::isfinite(w) || !(w > 0.0) || !std::isfinite(lo)) return 0.0;
+  size_t two_n = 2 * (size_t)N;
+  std::vector<double> hs(two_n), hdf(5 * two_n);
+  PointState st;
+  point_metric(s, ds, h, N, hs.data(), hdf.data(), st);
+  double g[10];
+  deformed_gradient(z, psr, psi, g);
+  int chart, elim;
+  double lo_unused;
+  chart_and_elim(z, g, chart, elim, lo_unused);
+  double fr[3][10];
+  affine_frame(g, chart, elim, fr);
+  C gt[3][3];
+  project_tangent(st.gamb, fr, gt);
+  double det = det3(gt);
+  if (!std::isfinite(det) || std::fabs(det) < 1e-30) return 0.0;
+  double log_eta = std::log(std::fabs(det)) - lo;
+  double eta = std::exp(log_eta);
+  if (!std::isfinite(eta) || !(eta > 0.0) || !std::isfinite(log_eta)) return 0.0;
+  // g_tan = L L^H (complex Cholesky of the 3x3 Hermitian matrix)
+  C L[3][3] = {};
+  for (int j = 0; j < 3; ++j) {
+    double dsum = gt[j][j].r;
+    for (int k = 0; k < j; ++k) dsum -= L[j][k].r * L[j][k].r + L[j][k].i * L[j][k].i;
+    if (!(dsum > 0.0) || !std::isfinite(dsum)) return 0.0;
+    double ljj = std::sqrt(dsum);
+    L[j][j] = {ljj, 0.0};
+    for (int i = j + 1; i < 3; ++i) {
+      C acc = gt[i][j];
+      for (int k = 0; k < j; ++k) acc = csub(acc, cmul(L[i][k], C{L[j][k].r, -L[j][k].i}));
+      L[i][j] = {acc.r / ljj, acc.i / ljj};
+    }
+  }
+  // B = L^{-1} T (3 x 5): e = B d f
+  C B[3][5];
+  for (int i = 0; i < 5; ++i)
+    for (int v = 0; v < 3; ++v) {
+      C acc = {fr[v][2 * i], fr[v][2 * i + 1]};
+      for (int u = 0; u < v; ++u) acc = csub(acc, cmul(L[v][u], B[u][i]));
+      B[v][i] = {acc.r / L[v][v].r, acc.i / L[v][v].r};
+    }
+  std::vector<C> sv(nd), dsv(5 * (size_t)nd);
+  small_basis(z, mono, nd, sv.data(), dsv.data());
+  double r2 = 0.0;
+  for (int j = 0; j < 5; ++j) r2 += z[2 * j] * z[2 * j] + z[2 * j + 1] * z[2 * j + 1];
+  const double S = d == 1 ? r2 : r2 * r2;
+  const double iS = 1.0 / S;
+  // d_i log S = d zbar_i / r2
+  C dlogS[5];
+  for (int i = 0; i < 5; ++i) dlogS[i] = {d * z[2 * i] / r2, -d * z[2 * i + 1] / r2};
+  for (int a = 0; a < nd; ++a)
+    for (int b = 0; b < nd; ++b) {
+      const int al = a * nd + b;
+      const C sbc = {sv[b].r, -sv[b].i};
+      const C fab = cmul(sv[a], sbc);
+      f[al] = {fab.r * iS, fab.i * iS};
+      C df[5];
+      for (int i = 0; i < 5; ++i) {  // d_i f = (d_i s_a) conj(s_b) / S - f d_i log S
+        C t1 = cmul(dsv[i * nd + a], sbc);
+        C t2 = cmul(f[al], dlogS[i]);
+        df[i] = {t1.r * iS - t2.r, t1.i * iS - t2.i};
+      }
+      for (int v = 0; v < 3; ++v) {
+        C acc = {0, 0};
+        for (int i = 0; i < 5; ++i) {
+          C c = cmul(B[v][i], df[i]);
+          acc = {acc.r + c.r, acc.i + c.i};
+        }
+        e[(size_t)v * nf + al] = acc;
+      }
+    }
+  return w * eta;
+}
+
+}  // namespace
+
+extern "C" {
+
+// Per-point Galerkin rows: f [P][nf] and e [P][3][nf] complex (interleaved), c [P].  Returns nf or -1.
+int orc_laplacian_rows(const double* s, const double* ds, const double* pts, const double* w, const double* log_om,
+                       size_t P, int N, double psr, double psi, const double* h_block, int d, double* F, double* E,
+                       double* c) {
+  if (d < 1 || d > 2) return -1;
+  std::vector<uint32_t> mono(5 * 64);
+  const int nd = orc_monomials(d, 0, mono.data());
+  const int nf = nd * nd;
+  const size_t two_n = 2 * (size_t)N;
+  parallel_for(P, [&](size_t p) {
+    c[p] = lap_point(s + p * two_n, ds + p * 5 * two_n, h_block, N, pts + p * 10, w[p], log_om[p], psr, psi,
+                     mono.data(), nd, d, reinterpret_cast<C*>(F + 2 * p * nf),
+                     reinterpret_cast<C*>(E + 2 * p * 3 * nf));
+  });
+  return nf;
+}
+
+// M, K (nf x nf complex, row-major, interleaved) from the rows of orc_laplacian_rows; serial point order.
+// Returns sum c (0 when no point is valid).
+double orc_laplacian_gram(const double* F, const double* E, const double* c, size_t P, int nf, double* Mout,
+                          double* Kout) {
+  const size_t n2 = (size_t)nf * nf;
+  std::vector<double> M(2 * n2, 0.0), K(2 * n2, 0.0);
+  double W = 0.0;
+  const C* Fc = reinterpret_cast<const C*>(F);
+  const C* Ec = reinterpret_cast<const C*>(E);
+  for (size_t p = 0; p < P; ++p) {
+    const double cp = c[p];
+    if (!(cp > 0.0)) continue;
+    W += cp;
+    const C* f = Fc + p * nf;
+    const C* e = Ec + p * 3 * nf;
+    for (int al = 0; al < nf; ++al) {
+      const C fa = {f[al].r, -f[al].i};
+      for (int be = 0; be < nf; ++be) {
+        const C m = cmul(fa, f[be]);
+        double kr = 0.0, ki = 0.0;
+        for (int v = 0; v < 3; ++v) {
+          const C ea = e[(size_t)v * nf + al], eb = e[(size_t)v * nf + be];
+          kr += ea.r * eb.r + ea.i * eb.i;
+          ki += ea.r * eb.i - ea.i * eb.r;
+        }
+        const size_t o = 2 * ((size_t)al * nf + be);
+        M[o] += cp * m.r;
+        M[o + 1] += cp * m.i;
+        K[o] += cp * kr;
+        K[o + 1] += cp * ki;
+      }
+    }
+  }
+  const double iw = W > 0 ? 1.0 / W : 0.0;
+  for (size_t i = 0; i < 2 * n2; ++i) {
+    Mout[i] = M[i] * iw;
+    Kout[i] = K[i] * iw;
+  }
+  return W;
+}
+
+// Y_ijk = sum_p w_p psi_i psi_j psi_k conj(Omega_p) / sum w over points with finite positive w,
+// psi_i = sum_al coeffs[i][al] f_al, Omega_p = z_chart / d_elim f (quintic.rs:4894-4909).
+// coeffs [n_modes][nf] complex; y [n_modes^3] complex.  Returns nf or -1.
+int orc_yukawa(const double* pts, const double* w, size_t P, double psr, double psi, int d, const double* coeffs,
+               int n_modes, double* y) {
+  if (d < 1 || d > 2 || n_modes < 1 || n_modes > 8) return -1;
+  std::vector<uint32_t> mono(5 * 64);
+  const int nd = orc_monomials(d, 0, mono.data());
+  const int nf = nd * nd;
+  const int n3 = n_modes * n_modes * n_modes;
+  std::vector<double> acc(2 * (size_t)n3, 0.0);
+  double W = 0.0;
+  std::vector<C> sv(nd), dsv(5 * (size_t)nd), ps(n_modes);
+  for (size_t p = 0; p < P; ++p) {
+    const double wp = w[p];
+    if (!std::isfinite(wp) || !(wp > 0.0)) continue;
+    const double* z = pts + p * 10;
+    double g[10];
+    deformed_gradient(z, psr, psi, g);
+    int chart, elim;
+    double lo;
+    chart_and_elim(z, g, chart, elim, lo);
+    const C ge = {g[2 * elim], g[2 * elim + 1]};
+    const double gn = ge.r * ge.r + ge.i * ge.i;
+    if (!(gn > 0.0)) continue;
+    const C om = cmul(C{z[2 * chart], z[2 * chart + 1]}, C{ge.r / gn, -ge.i / gn});
+    const C omc = {om.r, -om.i};
+    W += wp;
+    small_basis(z, mono.data(), nd, sv.data(), dsv.data());
+    double r2 = 0.0;
+    for (int j = 0; j < 5; ++j) r2 += z[2 * j] * z[2 * j] + z[2 * j + 1] * z[2 * j + 1];
+    const double iS = 1.0 / (d == 1 ? r2 : r2 * r2);
+    for (int i = 0; i < n_modes; ++i) {
+      C a = {0, 0};
+      for (int u = 0; u < nd; ++u)
+        for (int v = 0; v < nd; ++v) {
+          const int al = u * nd + v;
+          const C fab = cmul(sv[u], C{sv[v].r, -sv[v].i});
+          const C cc = {coeffs[2 * ((size_t)i * nf + al)], coeffs[2 * ((size_t)i * nf + al) + 1]};
+          const C t = cmul(cc, C{fab.r * iS, fab.i * iS});
+          a = {a.r + t.r, a.i + t.i};
+        }
+      ps[i] = a;
+    }
+    for (int i = 0; i < n_modes; ++i)
+      for (int j = 0; j < n_modes; ++j)
+        for (int k = 0; k < n_modes; ++k) {
+          const C t = cmul(cmul(cmul(ps[i], ps[j]), ps[k]), omc);
+          const size_t o = 2 * (((size_t)i * n_modes + j) * n_modes + k);
+          acc[o] += wp * t.r;
+          acc[o + 1] += wp * t.i;
+        }
+  }
+  const double iw = W > 0 ? 1.0 / W : 0.0;
+  for (size_t i = 0; i < acc.size(); ++i) y[i] = acc[i] * iw;
+  return nf;
+}
+
+}  // extern "C"
