@@ -80,3 +80,38 @@ def test_mixed_fs_gram_kat(cy, orc):
     m.orthonormalise_basis_fs_gram()
     m.donaldson_solve(rec["donaldson_iters_run"], 0.0)
     assert m.sigma() == pytest.approx(rec["sigma_donaldson"], rel=1e-6)
+
+
+# ---- sigma pass on the int8 tensor cores (Y = X . h with four 7-bit digits, exact int32 accumulation) ----
+# At a fixed h the split sigma pass must agree with the FP64 pass: sigma_L1 within 2e-8 relative,
+# sigma_L2^2 (a mean of squared deviations) within 5e-8, eta per point within 1e-6 relative (the
+# per-point metric carries ~2e-8 relative error at the worst points), the gradient of sigma_L2^2
+# within 1e-6 relative Frobenius.
+@pytest.mark.parametrize("k,psi,reduced,P", [(4, 0.5, False, 30000), (6, 0.1 + 0.2j, True, 40000),
+                                             (8, 0.1 + 0.2j, True, 12000)])
+def test_tensor_sigma_pass_matches_fp64(cy, orc, k, psi, reduced, P):
+    g = cy.QuinticSolver(k, P, 17, psi, reduced_basis=reduced)
+    for _ in range(3):
+        g.donaldson_step()
+    s64 = g.sigma()
+    eta64 = g.eta()
+    l2_64, gr64, _ = g.sigma_squared_and_gradient()
+    g.set_precision("fp16x3")
+    s16 = g.sigma()
+    eta16 = g.eta()
+    l2_16, gr16, _ = g.sigma_squared_and_gradient()
+    assert abs(s16 / s64 - 1) <= 2e-8
+    m = np.isfinite(eta64)
+    assert np.array_equal(m, np.isfinite(eta16))
+    assert np.max(np.abs(eta16[m] / eta64[m] - 1)) <= 1e-6
+    assert abs(l2_16 / l2_64 - 1) <= 5e-8
+    assert relf(gr16, gr64) <= 1e-6
+
+
+def test_tensor_sigma_minibatch_adam_tracks_fp64(cy, orc):
+    o = orc.OracleSolver.new_with_psi_sz(4, 20000, 5, 0.1 + 0.2j)
+    hist = {}
+    for prec in ("fp64", "fp16x3"):
+        g = cy.QuinticSolver.from_points(4, o.points, o.weights, o.log_omega_sq, psi=0.1 + 0.2j, precision=prec)
+        hist[prec] = np.array(g.sigma_refine_analytic(5, 1e-3, minibatch=8000, seed=3))
+    np.testing.assert_allclose(hist["fp16x3"], hist["fp64"], rtol=1e-8)
