@@ -49,6 +49,9 @@ def parse():
     ap.add_argument("--serving-rate", type=float, default=50.0)
     ap.add_argument("--serving-active", type=int, default=8)
     ap.add_argument("--galerkin-points", type=int, default=1_000_000, help="0 skips the Laplacian / Yukawa run")
+    ap.add_argument("--adam-points", type=int, default=2_000_000, help="0 skips the sigma-Adam run")
+    ap.add_argument("--adam-steps", type=int, default=200)
+    ap.add_argument("--adam-minibatch", type=int, default=200_000)
     return ap.parse_args()
 
 
@@ -281,6 +284,67 @@ def galerkin_run(a, dev, stream, h_block):
             "coefficients": "CN(0,1), numpy default_rng(seed), 3 x 225"}
 
 
+def adam_run(a, dev, stream):
+    """Config 3: sigma-functional Adam on the k=8 reduced basis (N=460), psi=0.1+0.2i, 2,000,000 points,
+    lr 1e-3, minibatch 200,000 drawn by a seeded permutation, from the h of five balancing steps.  The FP64
+    arm runs 10 steps from the same h; sigma and the gradient norm at the final h are compared with FP64
+    on a fixed 200,000-point subset."""
+    import torch
+
+    import papers_b200
+
+    psi = 0.1 + 0.2j
+    g = papers_b200.QuinticSolver.new_with_psi_sz(8, a.adam_points, a.seed + 2000, psi, reduced_basis=True,
+                                                  precision=a.precision, with_derivs=False, device=dev)
+    g.set_stream(stream.cuda_stream)
+    for _ in range(5):
+        g.donaldson_step()
+    h0 = g.h_block
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        out = fn()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        return out, ev0.elapsed_time(ev1)
+
+    g.profile(True)
+    g.profile_read(reset=True)
+    hist, ms = timed(lambda: g.sigma_refine_analytic(a.adam_steps, 1e-3, minibatch=a.adam_minibatch, seed=a.seed))
+    stages = {k: v[0] / max(v[1], 1) for k, v in g.profile_read(reset=True).items()}
+    g.profile(False)
+    h_final = g.h_block
+    n64 = min(10, a.adam_steps)
+    g.set_precision("fp64")
+    g.h_block = h0
+    hist64, ms64 = timed(lambda: g.sigma_refine_analytic(n64, 1e-3, minibatch=a.adam_minibatch, seed=a.seed))
+    pts, w, lo = g.get_points()
+    P = g.n_points
+    g.close()
+    m = min(a.adam_minibatch, P)
+    sub = papers_b200.QuinticSolver.from_points(8, pts[:m], w[:m], lo[:m], psi=psi, reduced_basis=True,
+                                                precision="fp64", device=dev)
+    sub.set_stream(stream.cuda_stream)
+    sub.h_block = h_final
+    l2_64, gr64, l1_64 = sub.sigma_squared_and_gradient()
+    sub.set_precision(a.precision)
+    l2_s, gr_s, l1_s = sub.sigma_squared_and_gradient()
+    sub.close()
+    h = np.asarray(hist)
+    return {"points": P, "n_basis": 460, "steps": len(hist), "minibatch": a.adam_minibatch, "lr": 1e-3,
+            "precision": a.precision, "ms": ms, "steps_per_s": len(hist) / (ms / 1e3),
+            "fp64_steps_per_s": n64 / (ms64 / 1e3), "speedup_vs_fp64": (len(hist) / ms) / (n64 / ms64),
+            "sigma_first": float(h[0]), "sigma_last": float(h[-1]),
+            "history_rel_diff_vs_fp64_first_steps": float(np.max(np.abs(h[:n64] / np.asarray(hist64) - 1))),
+            "at_final_h_on_subset": {"points": m, "sigma_l1_rel_err": abs(l1_s / l1_64 - 1),
+                                     "sigma_l2sq_rel_err": abs(l2_s / l2_64 - 1),
+                                     "grad_norm_rel_err": abs(np.linalg.norm(gr_s) / np.linalg.norm(gr64) - 1),
+                                     "grad_rel_frobenius": float(np.linalg.norm(gr_s - gr64) / np.linalg.norm(gr64))},
+            "stage_ms_per_call": stages}
+
+
 def run_reference(a, ws, rank):
     if rank != 0:
         return
@@ -366,7 +430,16 @@ def main():
 
     h_run = s.h_block
 
-    # ---- sigma evaluations per second ----
+    # ---- sigma evaluations per second; the first call on a point set also builds the digit planes of its
+    # section table (timed separately as setup) ----
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    s.sigma()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    sigma_setup_ms = dist_max(ev0.elapsed_time(ev1), ws)
+    s.profile(True)
+    s.profile_read(reset=True)
     torch.cuda.synchronize()
     ev0.record(stream)
     sig = None
@@ -376,9 +449,11 @@ def main():
     torch.cuda.synchronize()
     sigma_ms = dist_max(ev0.elapsed_time(ev1), ws)
     sigma_per_s = ws * a.sigma_steps / (sigma_ms / 1e3)
+    sigma_stages = {k: v[0] / max(v[1], 1) for k, v in s.profile_read(reset=True).items()}
+    s.profile(False)
 
     # ---- FP64 plain path on the same points: the 10x denominator and the accuracy reference ----
-    fp64_per_s, acc = None, None
+    fp64_per_s, acc, sigma64_per_s = None, None, None
     if a.precision != "fp64":
         s.set_precision("fp64")
         s.h_block = np.eye(2 * N)
@@ -391,6 +466,13 @@ def main():
         fp64_per_s = ws * a.steps / (dist_max(ev0.elapsed_time(ev1), ws) / 1e3)
         h64 = s.h_block
         sig64 = s.sigma()
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for _ in range(a.sigma_steps):
+            s.sigma()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        sigma64_per_s = ws * a.sigma_steps / (dist_max(ev0.elapsed_time(ev1), ws) / 1e3)
         acc = {"h_rel_frobenius": float(np.linalg.norm(h_run - h64) / np.linalg.norm(h64)),
                "sigma_fp64": sig64, "sigma_rel_err": abs(sig / sig64 - 1.0) if sig else None,
                "iterations": a.steps}
@@ -398,6 +480,7 @@ def main():
         s.h_block = h_run
     else:
         fp64_per_s = value
+        sigma64_per_s = sigma_per_s
 
     # ---- e2e through the C ABI from pinned host buffers ----
     pts, w, lo = s.get_points()
@@ -461,6 +544,11 @@ def main():
         barrier(ws)
         galerkin = galerkin_run(a, dev, stream, h_run)
 
+    adam = None
+    if a.adam_points > 0:
+        barrier(ws)
+        adam = adam_run(a, dev, stream)
+
     serving = None
     if a.serving_requests > 0:
         barrier(ws)
@@ -478,14 +566,15 @@ def main():
                                        f"(seeded LCG, GPU sampler), one Donaldson balancing iteration per step",
                            "precision": a.precision, "parallelism": f"replicas x{ws}",
                            "l2": "inputs larger than L2 (section table %.2f GB)" % (P * 6 * (2 * N + 30) * 8 / 1e9)},
-                "sigma_evals_per_s": sigma_per_s, "sigma": sig, "fp64_iters_per_s": fp64_per_s,
+                "sigma_evals_per_s": sigma_per_s, "sigma_evals_per_s_fp64": sigma64_per_s,
+                "sigma_setup_ms": sigma_setup_ms, "sigma": sig, "sigma_stage_ms": sigma_stages, "fp64_iters_per_s": fp64_per_s,
                 "accuracy_vs_fp64": acc,
                 "speedup_vs_fp64": (value / fp64_per_s) if fp64_per_s else None,
                 "residual_last": residuals[-1],
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                         "wall_s": e2e_wall},
                 "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu, "clocks": clocks,
-                "laplacian": galerkin, "serving": serving}
+                "laplacian": galerkin, "sigma_adam": adam, "serving": serving}
         print(json.dumps(line), flush=True)
     s.close()
     if ws > 1:
