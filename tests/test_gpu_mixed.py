@@ -115,3 +115,25 @@ def test_tensor_sigma_minibatch_adam_tracks_fp64(cy, orc):
         g = cy.QuinticSolver.from_points(4, o.points, o.weights, o.log_omega_sq, psi=0.1 + 0.2j, precision=prec)
         hist[prec] = np.array(g.sigma_refine_analytic(5, 1e-3, minibatch=8000, seed=3))
     np.testing.assert_allclose(hist["fp16x3"], hist["fp64"], rtol=1e-8)
+
+
+@pytest.mark.parametrize("k,P", [(3, 12000), (6, 40000)])
+def test_graph_replay_equals_eager(cy, orc, k, P):
+    """The step body replayed from CUDA graphs (the default) and launched eagerly (stage profiling on)
+    give bit-identical h and residuals, also across an externally set h (which refactors h)."""
+    psi = 0.1 + 0.2j
+    o = orc.OracleSolver.new_with_psi_sz(k, P, 21, psi, reduced=True)
+    g = cy.QuinticSolver.from_points(k, o.points, o.weights, o.log_omega_sq, psi=psi, reduced_basis=True,
+                                     precision="fp16x3")
+    e = cy.QuinticSolver.from_points(k, o.points, o.weights, o.log_omega_sq, psi=psi, reduced_basis=True,
+                                     precision="fp16x3")
+    e.profile(True)
+    for it in range(5):
+        if it == 3:
+            h = g.h_block
+            g.h_block = h
+            e.h_block = h
+        assert g.donaldson_step() == e.donaldson_step()
+        assert np.array_equal(g.h_block, e.h_block)
+    e.profile(False)
+    assert g.launch_count() > 0
