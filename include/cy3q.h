@@ -157,6 +157,24 @@ cy3q_status cy3q_laplacian_matrices(cy3q_solver* s, const cy3q_laplacian_config*
 cy3q_status cy3q_yukawa(cy3q_solver* s, const cy3q_laplacian_config* cfg, const double* coeffs, uint32_t n_modes,
                         double* y);
 
+/* ---- grouped balancing: one Donaldson step of many solves of different (psi, k, P) with the same
+        launches (no reference counterpart; each member's step is QuinticSolver::donaldson_step,
+        quintic.rs:428 / 1734-1894) ----
+   The tensor-core kernels of the step are persistent over a work list spanning all members and, with
+   the rest of the step, replayed from two CUDA graphs captured once per group (a membership change only
+   rewrites the group's tables).  Members are split-precision handles (fp16x3 / bf16x3) with points on
+   the group's device; the FP64 Cholesky of each T-operator runs between the two graphs.  A group is
+   used by one thread at a time (calls are serialised); its members must not be used elsewhere during a
+   call.  Each member's result equals its own cy3q_donaldson_step bit for bit. */
+typedef struct cy3q_group cy3q_group;
+/* capacity: the largest number of members per step (1 .. 1024) */
+cy3q_status cy3q_group_create(int32_t device, uint32_t capacity, cy3q_group** out);
+void cy3q_group_destroy(cy3q_group* g);
+/* One step of each of solvers[0 .. n): residuals[n] and statuses[n] (cy3q_status per member; a member
+   whose step failed keeps its previous h) may be NULL.  Returns the first member failure, or OK. */
+cy3q_status cy3q_group_step(cy3q_group* g, cy3q_solver* const* solvers, uint32_t n, double* residuals,
+                            int32_t* statuses);
+
 /* ---- serving: continuous batching of balancing solves on one GPU (no reference analogue; nearest is
         the toy crossbeam work queue, src/orchestrator.rs:1-120) ---- */
 typedef struct cy3q_server cy3q_server;
