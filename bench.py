@@ -195,6 +195,13 @@ def serving_stream(a, dev):
         psi = np.sqrt(u) * np.exp(2j * np.pi * v)
         reqs.append((t, dict(k=k, n_points=min(10 * N_REDUCED[k] ** 2, 2_000_000), seed=1000 + i, psi=psi,
                              iterations=10, precision=a.precision)))
+    # one solve of each request shape first, so that the autotuner's per-shape choice is made on an idle
+    # device (it is cached for the process) and not while the stream's solves run
+    for k in sorted({r["k"] for _, r in reqs}):
+        w = cy3q.QuinticSolver.new_with_psi_sz(k, min(10 * N_REDUCED[k] ** 2, 2_000_000), 1, 0.5, reduced_basis=True,
+                                               precision=a.precision, with_derivs=False, device=dev)
+        w.donaldson_step()
+        w.close()
     srv = cy3q.Server(dev, 0, a.serving_active)
     t0 = time.perf_counter()
     tickets = []
