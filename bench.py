@@ -530,30 +530,52 @@ def main():
     e2e_value = ws * a.steps / (e2e_ms / 1e3)
 
     # ---- roofline of the dominant stage ----
+    # Per launch of each tensor-core kernel of the split step (ldk = 2N rounded up to 64, Pp = P rounded up
+    # to 128): algorithmic flops 8 P N^2 (one complex contraction); algorithmic bytes: the Bergman kernel
+    # reads the split section rows X (hi + lo, Pp ldk 4 B) and writes the split T-operand Xt (Pp ldk 4 B);
+    # the T-operator reads Xt once (Pp ldk 4 B).  The binding roof is the one with the longer floor time
+    # (bytes / measured HBM copy bandwidth vs. 3 split products x flops / measured bf16 burst).
     pk, src = peaks()
     alg = algorithmic(P, N)
-    # DRAM bytes per point of the tensor-core kernels, from the ncu capture of the same kernels on a
-    # 100,096-point case (profiles/umma_*_k6.md), scaled linearly in points
-    traffic_per_point = {"bergman": (180.232192e6 + 6.467072e6) / 100096,
-                         "toperator": (179.593984e6 + 4.617472e6) / 100096}
+    ldk = -(-2 * N // 64) * 64
+    Pp = -(-P // 128) * 128
     stage_flops = {"toperator": alg["F_T"], "bergman": alg["F_K"]}
+    stage_bytes = {"bergman": 2.0 * Pp * ldk * 4, "toperator": 1.0 * Pp * ldk * 4}
+    # DRAM bytes per point of the two kernels, from the ncu captures of the same kernels on a 100,096-point
+    # case (profiles/umma_bergman_kernel_k6.md, profiles/umma_gram_kernel_toperator_k6.md), scaled in points
+    traffic_per_point = {"bergman": (290.958848e6 + 136.252928e6) / 100096,
+                         "toperator": (183.617792e6 + 25.158656e6) / 100096}
     cand = {k: v for k, v in stages.items() if k in stage_flops}
     dname, (dms, dcalls) = max(cand.items(), key=lambda kv: kv[1][0]) if cand else ("toperator", (ms, a.steps))
-    if a.precision == "fp64":
-        peak_tf, peak_note = 37.0, "nominal FP64 peak (MEASURED_PEAKS.json has no FP64 figure)"
-        traffic = None
-    else:
-        peak_tf, peak_note = pk["bf16_tflops"], f"{src} bf16 dense, burst (each kernel runs < 1 ms)"
-        traffic = traffic_per_point[dname] * P
     avg_ms = dms / max(dcalls, 1)
-    achieved = stage_flops[dname] / (avg_ms / 1e3) / 1e12
-    roof = {"bound": "tensor", "achieved": achieved, "peak": peak_tf, "unit": "TFLOP/s", "frac": achieved / peak_tf,
-            "traffic": traffic, "kernel_stage": dname, "avg_launch_ms": avg_ms, "peak_source": peak_note,
-            "algorithmic_flops_per_launch": stage_flops[dname],
-            "note": "achieved counts algorithmic flops (8PN^2 per GEMM); the split-precision tensor pipe executes "
-                    "3 products per flop on padded tiles, so the ceiling of frac is about 1/3",
-            "traffic_note": "DRAM bytes per launch scaled from the 100k-point ncu capture",
-            "stage_ms_per_step": {k: v[0] / max(v[1], 1) for k, v in stages.items()}}
+    if a.precision == "fp64":
+        roof = {"bound": "fp64", "achieved": stage_flops[dname] / (avg_ms / 1e3) / 1e12, "peak": 37.0,
+                "unit": "TFLOP/s", "peak_source": "nominal FP64 peak (MEASURED_PEAKS.json has no FP64 figure)",
+                "traffic": None}
+        roof["frac"] = roof["achieved"] / roof["peak"]
+    else:
+        hbm, tf = pk["hbm_gbs"], pk["bf16_tflops"]
+        floor_hbm_ms = stage_bytes[dname] / (hbm * 1e9) * 1e3
+        floor_tensor_ms = 3.0 * stage_flops[dname] / (tf * 1e12) * 1e3
+        tensor_view = {"achieved": stage_flops[dname] / (avg_ms / 1e3) / 1e12, "peak": tf, "unit": "TFLOP/s",
+                       "floor_ms": floor_tensor_ms,
+                       "note": "algorithmic flops (8PN^2); the fp16x3 split runs 3 MMA products per flop, so "
+                               "the ceiling of achieved / peak is 1/3"}
+        tensor_view["frac"] = tensor_view["achieved"] / tf
+        hbm_view = {"achieved": stage_bytes[dname] / (avg_ms / 1e3) / 1e9, "peak": hbm, "unit": "GB/s",
+                    "floor_ms": floor_hbm_ms, "algorithmic_bytes_per_launch": stage_bytes[dname]}
+        hbm_view["frac"] = hbm_view["achieved"] / hbm
+        main = hbm_view if floor_hbm_ms >= floor_tensor_ms else tensor_view
+        roof = {"bound": "hbm" if main is hbm_view else "tensor", "achieved": main["achieved"], "peak": main["peak"],
+                "unit": main["unit"], "frac": main["frac"], "traffic": traffic_per_point[dname] * P,
+                "peak_source": f"{src} (MEASURED_PEAKS.json: HBM copy GB/s, bf16 dense burst TF/s; each kernel runs "
+                               f"< 1 ms)",
+                "hbm_view": hbm_view, "tensor_view": tensor_view}
+    roof.update({"kernel_stage": dname, "avg_launch_ms": avg_ms,
+                 "kernel": {"bergman": "umma_bergman_kernel", "toperator": "umma_gram_kernel"}[dname],
+                 "algorithmic_flops_per_launch": stage_flops[dname],
+                 "traffic_note": "DRAM bytes per launch scaled from the 100k-point ncu capture",
+                 "stage_ms_per_step": {k: v[0] / max(v[1], 1) for k, v in stages.items()}})
 
     galerkin = None
     if a.galerkin_points > 0:
