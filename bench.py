@@ -590,7 +590,10 @@ def main():
     serving = None
     if a.serving_requests > 0:
         barrier(ws)
-        serving = serving_stream(a, dev)
+        try:
+            serving = serving_stream(a, dev)
+        except Exception as exc:  # the balancing line above is complete; report the failed section in it
+            serving = {"error": f"{type(exc).__name__}: {exc}"[:500]}
 
     cpu = None
     if rank == 0 and ws == 1 and not a.no_cpu_baseline:
@@ -614,7 +617,11 @@ def main():
                 "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu, "clocks": clocks,
                 "laplacian": galerkin, "sigma_adam": adam, "serving": serving}
         print(json.dumps(line), flush=True)
-    s.close()
+    try:
+        s.close()
+    except Exception:
+        if not (serving and "error" in serving):  # a device fault in serving already is in the line
+            raise
     if ws > 1:
         import torch.distributed as dist
 
