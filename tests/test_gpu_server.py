@@ -73,7 +73,8 @@ def test_server_matches_solver(cy):
 
 def test_cancel_timeout_and_budget(cy):
     srv = cy.Server(0, 0, 1)
-    long_t = srv.submit(k=6, n_points=400000, seed=1, psi=0.5, iterations=400, precision="fp16x3")
+    # long enough that the cancel below always lands while it runs (it ends at the next iteration)
+    long_t = srv.submit(k=6, n_points=400000, seed=1, psi=0.5, iterations=100000, precision="fp16x3")
     queued = srv.submit(k=3, n_points=5000, seed=2, psi=0.5, iterations=2)
     # deadline: the long request cannot finish within 1 ms
     with pytest.raises(cy.Cy3qError) as e:
@@ -83,7 +84,7 @@ def test_cancel_timeout_and_budget(cy):
     assert srv.wait(queued, 10000).status == cy.ERR_CANCELLED
     srv.cancel(long_t)  # running: stops between iterations
     res = srv.wait(long_t, 120000)
-    assert res.status == cy.ERR_CANCELLED and res.iterations < 400
+    assert res.status == cy.ERR_CANCELLED and res.iterations < 100000
     st = srv.stats()
     assert st["cancelled"] == 2 and st["hbm_in_use"] == 0
     srv.close()
