@@ -512,7 +512,7 @@ def main():
         e.set_points(hp.numpy(), hw.numpy(), hl.numpy())
         for _ in range(a.steps):
             e.donaldson_step()
-        h_out[:] = e.h_block
+        e.get_h(out=h_out)
 
     e2e_run()  # warm: device buffers of the handle are allocated once and reused
     torch.cuda.synchronize()
