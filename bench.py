@@ -408,7 +408,11 @@ def main():
                                                   precision=a.precision, with_derivs=True, device=dev)
     s.set_stream(stream.cuda_stream)
     P, N = s.n_points, s.n_basis
-    for _ in range(a.warmup):
+    # warm-up covers both paths of the timed region: the first step after an externally set h (one
+    # refactorisation, whose library kernels load on first use) and the graph-replayed steps
+    for i in range(a.warmup):
+        if i == 0:
+            s.h_block = np.eye(2 * N)
         s.donaldson_step()
     s.h_block = np.eye(2 * N)
 

@@ -56,6 +56,22 @@ def test_sections_bitwise_on_identical_points(cy, orc):
     np.testing.assert_array_equal(g.section_values, o.section_values)
 
 
+def test_points_uploaded_in_pieces_bitwise(cy, orc):
+    """70,001 points take the upload in four uneven pieces, each piece's point measure and section rows
+    running as soon as it lands: the table is bit-identical to the oracle's, and weights and log|Omega|^2
+    computed piece by piece equal those of the one-piece upload of fewer points."""
+    o = _orc_set(orc, 3, 70001, 5, 0.5)
+    g = cy.QuinticSolver.from_points(3, o.points, o.weights, o.log_omega_sq, psi=0.5)
+    np.testing.assert_array_equal(g.section_values, o.section_values)
+    g2 = cy.QuinticSolver.from_points(3, o.points, psi=0.5)
+    small = cy.QuinticSolver.from_points(3, o.points[:30000], psi=0.5)
+    _, w2, lo2 = g2.get_points()
+    _, ws, los = small.get_points()
+    np.testing.assert_array_equal(w2[:30000], ws)
+    np.testing.assert_array_equal(lo2[:30000], los)
+    np.testing.assert_allclose(w2, o.weights, rtol=1e-9)
+
+
 @pytest.mark.parametrize("k,psi,reduced", [(3, 0.0, False), (4, 0.5, False), (6, 0.1 + 0.2j, True)])
 def test_donaldson_fp64_parity(cy, orc, k, psi, reduced):
     P = 20000 if k < 6 else 12000
