@@ -43,7 +43,6 @@ def parse():
     ap.add_argument("--psi", type=float, default=0.5)
     ap.add_argument("--seed", type=int, default=42)
     ap.add_argument("--sigma-steps", type=int, default=5)
-    ap.add_argument("--cpu-sample", type=int, default=25_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--serving-requests", type=int, default=256, help="0 skips the serving stream")
     ap.add_argument("--serving-rate", type=float, default=50.0)
@@ -157,22 +156,19 @@ def peaks():
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
 
 
-def cpu_baseline(pts, w, lo, k, psi, n_full, sample, reduced=True):
-    """Balancing iteration of the FP64 oracle port on the host cores, on a bounded sample of the same
-    points; scaled linearly in points to the full workload."""
+def cpu_baseline(pts, w, lo, k, psi, reduced=True):
+    """One balancing iteration of the FP64 oracle port on the host cores over every point of the workload
+    (no scaling): per-point K threaded, the T-operator sum serial, as in the reference."""
     import oracle
 
     oracle.set_threads(os.cpu_count() or 1)
-    n = min(sample, len(pts))
-    o = oracle.OracleSolver(pts[:n], w[:n], lo[:n], oracle.monomials(k, reduced), psi, k)
+    o = oracle.OracleSolver(pts, w, lo, oracle.monomials(k, reduced), psi, k, with_derivs=False)
     t0 = time.perf_counter()
     o.donaldson_step()
     dt = time.perf_counter() - t0
-    per_full = dt * (n_full / n)
-    return {"value": 1.0 / per_full, "unit": UNIT, "cores": oracle.threads(), "kind": "port",
-            "sample": f"1 FP64 balancing iteration on {n} of the {n_full} points (k={k}, N={o.n_basis}), "
-                      f"{dt:.2f} s, scaled linearly to {n_full} points; per-point K threaded, T-operator sum "
-                      f"serial as in the reference"}
+    return {"value": 1.0 / dt, "unit": UNIT, "cores": oracle.threads(), "kind": "port",
+            "sample": f"1 FP64 balancing iteration over all {len(pts)} points (k={k}, N={o.n_basis}), {dt:.2f} s; "
+                      f"per-point K threaded, T-operator sum serial as in the reference"}
 
 
 N_REDUCED = {2: 15, 3: 35, 4: 70, 5: 125, 6: 205, 7: 315, 8: 460}
@@ -353,18 +349,20 @@ def adam_run(a, dev, stream):
 
 
 def run_reference(a, ws, rank):
+    """The reference's CPU path (its Rust crate cannot be built here: no toolchain and its first-party
+    dependency pwos-math is absent), as the oracle's FP64 port of it, on the whole workload: the same
+    500,000 points, W untimed and K timed Donaldson iterations, every host core."""
     if rank != 0:
         return
     import oracle
 
     oracle.build()
     # identical synthetic points to our arm (oracle sampler, same seed / psi)
-    n = a.cpu_sample
-    pts, _ = oracle.sample_sz(n, a.seed, a.psi, fermat_variant=False)
+    pts, _ = oracle.sample_sz(a.points, a.seed, a.psi, fermat_variant=False)
     w = oracle.weights(pts, a.psi)
     lo, _, _ = oracle.log_omega(pts, a.psi)
     oracle.set_threads(os.cpu_count() or 1)
-    o = oracle.OracleSolver(pts, w, lo, oracle.monomials(a.k, True), a.psi, a.k)
+    o = oracle.OracleSolver(pts, w, lo, oracle.monomials(a.k, True), a.psi, a.k, with_derivs=False)
     for _ in range(max(a.warmup, 0)):
         o.donaldson_step()
     o.h_block = np.eye(2 * o.n_basis)
@@ -372,24 +370,39 @@ def run_reference(a, ws, rank):
     for _ in range(a.steps):
         o.donaldson_step()
     dt = time.perf_counter() - t0
-    scale = a.points / n
-    v = a.steps / (dt * scale)
+    v = a.steps / dt
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": a.gpus, "steps": a.steps,
-            "warmup": a.warmup, "ms_per_step": 1e3 * dt * scale / a.steps, "higher_is_better": True,
+            "warmup": a.warmup, "ms_per_step": 1e3 * dt / a.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"Dwork psi={a.psi} k={a.k} reduced N={o.n_basis}, {a.points} line-intersection "
+            "config": {"workload": f"Dwork psi={a.psi} k={a.k} reduced N={o.n_basis}, {len(pts)} line-intersection "
                                    f"points, one Donaldson iteration per step", "precision": "fp64",
                        "l2": "inputs larger than L2"},
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": oracle.threads(), "kind": "port",
-                             "sample": f"each step runs on {n} of the {a.points} points (oracle FP64 port of the "
-                                       f"reference Rust path), scaled linearly in points"},
+                             "sample": f"{a.steps} timed iterations over all {len(pts)} points after {a.warmup} "
+                                       f"untimed ones (oracle FP64 port of the reference Rust path)"},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
+def relaunch_under_torchrun(a):
+    """`--gpus N` with N > 1 outside torchrun: start N ranks (one per GPU) the way the driver does."""
+    import socket
+
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={a.gpus}",
+           "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.abspath(__file__), *sys.argv[1:]]
+    os.execv(sys.executable, cmd)
+
+
 def main():
     a = parse()
+    if a.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        relaunch_under_torchrun(a)
     ws, rank, local = dist_setup()
+    if ws != a.gpus:
+        raise SystemExit(f"--gpus {a.gpus} does not match the {ws} ranks started by torchrun")
     if a.impl == "reference":
         run_reference(a, ws, rank)
         return
@@ -545,8 +558,8 @@ def main():
     Pp = -(-P // 128) * 128
     stage_flops = {"toperator": alg["F_T"], "bergman": alg["F_K"]}
     stage_bytes = {"bergman": 2.0 * Pp * ldk * 4, "toperator": 1.0 * Pp * ldk * 4}
-    # DRAM bytes per point of the two kernels, from the ncu captures of the same kernels on a 100,096-point
-    # case (profiles/umma_bergman_kernel_k6.md, profiles/umma_gram_kernel_toperator_k6.md), scaled in points
+    # DRAM bytes per point of the two kernels (dram__bytes_read.sum + dram__bytes_write.sum of one ncu capture of
+    # each kernel on a 100,096-point case of this workload), scaled in points: both stream their operands once
     traffic_per_point = {"bergman": (290.958848e6 + 136.252928e6) / 100096,
                          "toperator": (183.617792e6 + 25.158656e6) / 100096}
     cand = {k: v for k, v in stages.items() if k in stage_flops}
@@ -601,25 +614,38 @@ def main():
 
     cpu = None
     if rank == 0 and ws == 1 and not a.no_cpu_baseline:
-        cpu = cpu_baseline(pts, w, lo, a.k, psi, P, a.cpu_sample)
+        cpu = cpu_baseline(pts, w, lo, a.k, psi)
 
     if rank == 0:
+        # the per-stage maps and the full section records go to stderr as one JSON object; the result line on
+        # stdout keeps scalars, so that it stays short and the accuracy figures sit at its end
+        detail = {"stage_ms_per_step": roof.pop("stage_ms_per_step", None), "hbm_view": roof.pop("hbm_view", None),
+                  "tensor_view": roof.pop("tensor_view", None), "sigma_stage_ms": sigma_stages,
+                  "laplacian": galerkin, "sigma_adam": adam, "serving": serving}
+        print("bench detail: " + json.dumps(detail), file=sys.stderr, flush=True)
+
+        def pick(d, keys):
+            return None if d is None else {k: d.get(k) for k in keys if k in d}
+
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": a.steps, "warmup": a.warmup,
                 "ms_per_step": ms_max / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f64" if a.precision == "fp64" else a.precision, "data": "synthetic",
-                "config": {"workload": f"Dwork psi={a.psi} k={a.k} reduced N={N}, {P} line-intersection points "
-                                       f"(seeded LCG, GPU sampler), one Donaldson balancing iteration per step",
+                "config": {"workload": f"Dwork psi={a.psi} k={a.k} N={N}, {P} pts, 1 balancing iteration/step",
                            "precision": a.precision, "parallelism": f"replicas x{ws}",
                            "l2": "inputs larger than L2 (section table %.2f GB)" % (P * 6 * (2 * N + 30) * 8 / 1e9)},
-                "sigma_evals_per_s": sigma_per_s, "sigma_evals_per_s_fp64": sigma64_per_s,
-                "sigma_setup_ms": sigma_setup_ms, "sigma": sig, "sigma_stage_ms": sigma_stages, "fp64_iters_per_s": fp64_per_s,
-                "accuracy_vs_fp64": acc,
-                "speedup_vs_fp64": (value / fp64_per_s) if fp64_per_s else None,
-                "residual_last": residuals[-1],
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                         "wall_s": e2e_wall},
                 "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu, "clocks": clocks,
-                "laplacian": galerkin, "sigma_adam": adam, "serving": serving}
+                "laplacian": pick(galerkin, ["ms", "fp64_ms", "eig_max_rel_err_vs_fp64", "yukawa_ms"]),
+                "sigma_adam": pick(adam, ["steps_per_s", "fp64_steps_per_s"]) if adam else None,
+                "sigma_adam_err": pick((adam or {}).get("at_final_h_on_subset"),
+                                       ["sigma_l1_rel_err", "grad_rel_frobenius"]) if adam else None,
+                "serving": pick(serving, ["error", "failed", "p50_ms", "p99_ms", "iters_per_s",
+                                          "fp64_one_at_a_time_iters_per_s"]),
+                "residual_last": residuals[-1], "sigma": sig,
+                "sigma_evals_per_s": sigma_per_s, "sigma_evals_per_s_fp64": sigma64_per_s,
+                "fp64_iters_per_s": fp64_per_s, "speedup_vs_fp64": (value / fp64_per_s) if fp64_per_s else None,
+                "accuracy_vs_fp64": pick(acc, ["h_rel_frobenius", "sigma_rel_err", "iterations"])}
         print(json.dumps(line), flush=True)
     try:
         s.close()

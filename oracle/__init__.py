@@ -229,7 +229,7 @@ def identity_h(N: int) -> np.ndarray:
 class OracleSolver:
     """Mirror of the reference workspace `QuinticSolver` (quintic.rs:117-165) on the oracle."""
 
-    def __init__(self, points, weights_, log_om, monomials_, psi=0.0, k_degree=None):
+    def __init__(self, points, weights_, log_om, monomials_, psi=0.0, k_degree=None, with_derivs=True):
         self.points = np.ascontiguousarray(points, dtype=np.float64)
         self.n_points = len(self.points)
         self.weights = np.ascontiguousarray(weights_, dtype=np.float64)
@@ -239,7 +239,8 @@ class OracleSolver:
         self.k_degree = k_degree
         self.psi = complex(psi)
         self.section_values = basis(self.points, self.monomials)
-        self.section_derivs = basis_derivs(self.points, self.monomials)
+        # the balancing step needs the values only; sigma and its gradient need the derivatives too
+        self.section_derivs = basis_derivs(self.points, self.monomials) if with_derivs else None
         self.h_block = identity_h(self.n_basis)
         self.donaldson_residuals: list[float] = []
 
@@ -268,7 +269,7 @@ class OracleSolver:
     # methods
     def orthonormalise_basis_fs_gram(self):
         """quintic.rs:3140."""
-        rc = lib().orc_fs_gram_orthonormalise(self.section_values.reshape(-1), self.section_derivs.ctypes.data,
+        rc = lib().orc_fs_gram_orthonormalise(self.section_values.reshape(-1), None if self.section_derivs is None else self.section_derivs.ctypes.data,
                                               self.weights, self.n_points, self.n_basis)
         if rc != 0:
             raise ValueError("FS Gram matrix not positive-definite")

@@ -177,3 +177,61 @@ def test_error_paths(cy):
     with pytest.raises(Cy3qError) as e:
         cy.QuinticSolver(3, 200000, 1, hbm_budget_bytes=1 << 20)
     assert "OOM" in str(e.value)
+
+
+def test_config1_fermat_k3_fresh_sigma(cy, orc):
+    """Configuration 1 as written: Fermat quintic, k = 3 (N = 35), 20,000 line-intersection points, 10
+    Donaldson iterations from h = I, then sigma on 20,000 fresh points sampled with seed 0.  The GPU runs
+    it end to end (its own sampler, cy3q_sigma_on_points for the fresh set); the oracle runs the same
+    protocol.  h and both sigmas within 1e-10."""
+    g = cy.QuinticSolver.new_with_sampler(3, 20000, 42, 1e-12, "sz")
+    o = orc.OracleSolver.new_with_sampler(3, 20000, 42, 1e-12, "sz")
+    for _ in range(10):
+        g.donaldson_step()
+        o.donaldson_step()
+    assert relf(g.h_block, o.h_block) <= 1e-10
+    assert g.sigma() == pytest.approx(o.sigma(), rel=1e-10)
+    fresh = orc.OracleSolver.new_with_sampler(3, 20000, 0, 1e-12, "sz")
+    fresh.h_block = o.h_block.copy()
+    s_fresh_o = fresh.sigma()
+    # points only: the library derives weights and log|Omega|^2 from them, as the reference does
+    assert g.sigma_on_points(fresh.points) == pytest.approx(s_fresh_o, rel=1e-10)
+    assert g.sigma_on_points(fresh.points, fresh.weights, fresh.log_omega_sq) == pytest.approx(s_fresh_o, rel=1e-10)
+
+
+@pytest.mark.parametrize("psi", [0.0, 0.5, 0.1 + 0.2j])
+def test_newton_polish_matches_oracle(cy, orc, psi):
+    """FP64 Newton polish of every root on its line (3 steps after the Durand-Kerner sweeps): the GPU
+    sampler and the oracle keep the same points to 1e-12."""
+    P = 20000
+    g = cy.QuinticSolver(3, P, 19, psi, fermat_variant=(psi == 0), newton_polish=3)
+    pts_o, _ = orc.sample_sz(P, 19, psi, fermat_variant=(psi == 0), newton_iters=3)
+    pts_u, _ = orc.sample_sz(P, 19, psi, fermat_variant=(psi == 0), newton_iters=0)
+    pts, w, lo = g.get_points()
+    assert pts.shape == pts_o.shape
+    assert np.max(np.abs(pts - pts_o)) < 1e-12
+    # the polish changes the roots (the residual |f| on the polished points is no larger)
+    assert np.max(np.abs(pts_o - pts_u)) > 0
+    f_pol = max(abs(orc.quintic_value(p, psi)) for p in pts_o[:500])
+    f_raw = max(abs(orc.quintic_value(p, psi)) for p in pts_u[:500])
+    assert f_pol <= f_raw
+    np.testing.assert_allclose(w, orc.weights(pts_o, psi), rtol=1e-9)
+
+
+def test_asymmetric_external_h_fp64(cy, orc):
+    """An h_block set from outside that is not exactly symmetric: K_p = s^T h s is taken over the whole
+    block, as the reference does (quintic.rs:1744-1758), so one FP64 step matches the oracle."""
+    o = _orc_set(orc, 3, 12000, 23, 0.5)
+    g = cy.QuinticSolver.from_points(3, o.points, o.weights, o.log_omega_sq, psi=0.5)
+    for _ in range(2):
+        o.donaldson_step()
+        g.donaldson_step()
+    rng = np.random.default_rng(4)
+    h = o.h_block.copy()
+    h += 1e-3 * np.abs(h).max() * rng.standard_normal(h.shape) * (rng.random(h.shape) < 0.2)
+    assert np.abs(h - h.T).max() > 0
+    o.h_block = h.copy()
+    g.h_block = h
+    ro, rg = o.donaldson_step(), g.donaldson_step()
+    assert rg == pytest.approx(ro, rel=1e-10)
+    assert relf(g.h_block, o.h_block) <= 1e-10

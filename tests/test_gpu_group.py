@@ -97,3 +97,32 @@ def test_group_capacity_and_arguments(cy, clouds):
     with pytest.raises(cy.Cy3qError):
         g.step([f])  # FP64 handles are not grouped
     g.close()
+
+
+# Large bases next to small ones: k = 7 (N = 315, 2N mod 128 = 118, ldk 640, T-operator tail of 128
+# columns) and k = 8 (N = 460, 2N mod 128 = 24, ldk 960, tail of 32 columns, 36 T tiles) at reduced point
+# counts, mixed with k = 2..4 in one group whose capacity is larger than any earlier membership, so the
+# tables grow while members of every width share them.
+LARGE = [(2, 0.3 + 0.4j, 3000, 51), (7, 0.2 - 0.1j, 30000, 52), (3, 0.5, 20000, 53), (8, 0.1 + 0.2j, 30000, 54),
+         (4, -0.4 + 0.1j, 20000, 55)]
+
+
+def _sampled(cy, k, psi, P, seed):
+    return cy.QuinticSolver.new_with_psi_sz(k, P, seed, psi, reduced_basis=True, precision="fp16x3",
+                                            with_derivs=False)
+
+
+def test_group_large_bases_mix_equals_alone(cy):
+    alone = [_sampled(cy, *x) for x in LARGE]
+    grouped = [_sampled(cy, *x) for x in LARGE]
+    assert [s.n_basis for s in grouped] == [15, 315, 35, 460, 70]
+    g = cy.Group(0, capacity=6)
+    schedule = [[0, 2], [0, 1, 2], [1, 3], [0, 1, 2, 3, 4], [3, 4], [0, 1, 2, 3, 4]]
+    for members in schedule:
+        res, st = g.step([grouped[i] for i in members])
+        assert list(st) == [0] * len(members)
+        for j, i in enumerate(members):
+            assert res[j] == alone[i].donaldson_step(), (members, i)
+    for a, b in zip(alone, grouped):
+        assert np.array_equal(a.h_block, b.h_block)
+    g.close()

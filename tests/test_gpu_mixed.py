@@ -137,3 +137,20 @@ def test_graph_replay_equals_eager(cy, orc, k, P):
         assert np.array_equal(g.h_block, e.h_block)
     e.profile(False)
     assert g.launch_count() > 0
+
+
+def test_config2_full_size_accuracy(cy):
+    """Configuration 2 at its full size: Dwork psi = 0.5, k = 6 reduced (N = 205), 500,000 GPU-sampled
+    points, 20 balancing iterations from h = I in fp16x3 against the FP64 path on the same points.  The
+    north star's bar: sigma within 1e-6 relative; h within 2e-6 relative Frobenius."""
+    f = cy.QuinticSolver.new_with_psi_sz(6, 500000, 42, 0.5, reduced_basis=True, with_derivs=True)
+    pts, w, lo = f.get_points()
+    m = cy.QuinticSolver.from_points(6, pts, w, lo, psi=0.5, reduced_basis=True, precision="fp16x3")
+    for _ in range(20):
+        f.donaldson_step()
+        m.donaldson_step()
+    assert relf(m.h_block, f.h_block) < 2e-6
+    sf = f.sigma()
+    assert m.sigma() == pytest.approx(sf, rel=1e-6)
+    f.close()
+    m.close()

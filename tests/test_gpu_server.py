@@ -93,3 +93,34 @@ def test_cancel_timeout_and_budget(cy):
         small.submit(k=6, n_points=400000, seed=1, psi=0.5)
     assert "ERR_OOM" in str(e.value)
     small.close()
+
+
+def test_large_bases_in_the_mix_equal_alone(cy):
+    """k = 7 and k = 8 requests (N = 315 and 460) at reduced point counts share the grouped steps with
+    k = 2..4 requests; every request's h and residual equal the same request served alone, bit for bit."""
+    rng = np.random.default_rng(11)
+    reqs = []
+    for i, k in enumerate([2, 8, 3, 7, 4, 2, 8, 3, 7]):
+        u, v = rng.random(), rng.random()
+        psi = np.sqrt(u) * 0.9 * np.exp(2j * np.pi * v)
+        n = {2: 15, 3: 35, 4: 70, 7: 315, 8: 460}[k]
+        reqs.append(dict(k=k, n_points=min(10 * n * n, 30000), seed=300 + i, psi=psi, iterations=3,
+                         precision="fp16x3"))
+    srv = cy.Server(0, 0, 4)
+    tickets = [srv.submit(**r) for r in reqs]
+    mix = []
+    for t in tickets:
+        res = srv.wait(t, 300000)
+        assert res.status == 0
+        mix.append((res.residual, srv.h_block(t, res.n_basis)))
+    st = srv.stats()
+    assert st["completed"] == len(reqs) and st["failed"] == 0 and st["hbm_in_use"] == 0
+    srv.close()
+    alone = cy.Server(0, 0, 1)
+    for r, (res_m, h_m) in zip(reqs, mix):
+        t = alone.submit(**r)
+        res_a = alone.wait(t, 300000)
+        assert res_a.status == 0
+        assert res_a.residual == res_m, r
+        assert np.array_equal(alone.h_block(t, res_a.n_basis), h_m), r
+    alone.close()

@@ -6,7 +6,9 @@ or a loop that cannot afford the device-wide synchronisation a cudaMalloc / cuda
 Such a caller owns every device buffer; the library keeps its intermediates in one fixed device
 array.  Here the test plays that caller: it allocates the inputs and the eta output itself (with
 torch) and checks, on two calls in a row, that the result equals the allocating path (cy3q_sigma
-through a solver handle) to the parity tolerance of the FP64 tests (1e-10 relative).
+through a solver handle) and the FP64 oracle to the parity tolerance of the FP64 tests (1e-10 relative),
+and that the second call changes neither the device's free memory, nor the reserved and used bytes of
+the default stream-ordered memory pool, nor torch's allocated bytes.
 
 This file is collected last so that a run stopping at the first failure has run every other test.
 """
@@ -28,6 +30,31 @@ def cy():
     import papers_b200
 
     return papers_b200
+
+
+def _device_memory(dev):
+    """Free device bytes, the default memory pool's reserved and used bytes, and torch's allocated bytes."""
+    import torch
+
+    free, _ = torch.cuda.mem_get_info(dev)
+    pool = (None, None)
+    try:
+        from cuda.bindings import runtime as rt
+    except ImportError:  # older cuda-python layout
+        try:
+            from cuda import cudart as rt
+        except ImportError:
+            rt = None
+    if rt is not None:
+        err, p = rt.cudaDeviceGetDefaultMemPool(dev.index)
+        if int(err) == 0:
+            vals = []
+            for attr in (rt.cudaMemPoolAttr.cudaMemPoolAttrReservedMemCurrent,
+                         rt.cudaMemPoolAttr.cudaMemPoolAttrUsedMemCurrent):
+                e2, v = rt.cudaMemPoolGetAttribute(p, attr)
+                vals.append(int(v) if int(e2) == 0 else None)
+            pool = tuple(vals)
+    return free, pool, torch.cuda.memory_allocated(dev)
 
 
 def _call(L, k, reduced, psi, dp, dw, dlo, P, dh, deta, stream):
@@ -58,16 +85,27 @@ def test_sigma_noalloc_matches_sigma_twice(cy, orc, k, psi, reduced):
     dlo = torch.from_numpy(o.log_omega_sq.copy()).to(dev)
     dh = torch.from_numpy(np.ascontiguousarray(h)).to(dev)
     stream = torch.cuda.current_stream(dev).cuda_stream
+    detas = [torch.full((P,), float("nan"), dtype=torch.float64, device=dev) for _ in range(2)]
+    torch.cuda.synchronize()
+    mem, out = [], []
     for call in range(2):
-        deta = torch.full((P,), float("nan"), dtype=torch.float64, device=dev)
+        out.append(_call(L, k, reduced, complex(psi), dp, dw, dlo, P, dh, detas[call], stream))
         torch.cuda.synchronize()
-        st, sig = _call(L, k, reduced, complex(psi), dp, dw, dlo, P, dh, deta, stream)
+        mem.append(_device_memory(dev))
+    o.h_block = np.ascontiguousarray(h)
+    s_orc = o.sigma()
+    assert s_ref == pytest.approx(s_orc, rel=TOL)
+    for call, (st, sig) in enumerate(out):
         assert st == 0, cy3q._err(None)
         assert sig == pytest.approx(s_ref, rel=TOL), call
-        eta = deta.cpu().numpy()
+        assert sig == pytest.approx(s_orc, rel=TOL), call
+        eta = detas[call].cpu().numpy()
         m = np.isfinite(eta_ref)
         assert np.array_equal(m, np.isfinite(eta)), call
         np.testing.assert_allclose(eta[m], eta_ref[m], rtol=TOL)
+    # the contract itself: the second call (after the first has loaded the kernels) allocated no device
+    # memory, neither from the driver nor from the stream-ordered pool nor from torch's allocator
+    assert mem[1] == mem[0], mem
 
 
 def test_sigma_noalloc_rejects_basis_beyond_limit(cy):
