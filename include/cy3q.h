@@ -128,6 +128,19 @@ cy3q_status cy3q_sigma_grad(cy3q_solver* s, double* sigma_l2sq, double* grad, do
    seeded permutation.  history[steps] receives sigma_L1 before each update; *steps_done the count. */
 cy3q_status cy3q_adam_refine(cy3q_solver* s, int32_t steps, double lr, uint64_t minibatch, uint64_t seed,
                              double* history, int32_t* steps_done);
+/* QuinticSolver::sigma_refine_lbfgs_gpu_legacy (quintic.rs:678-890; sigma_refine_lbfgs_gpu, quintic.rs:901,
+   follows the same trajectory): L-BFGS on [h_re ; h_im] minimising sigma_L2^2 with the analytic gradient,
+   m_history pairs, backtracking Armijo search with a steepest-descent fallback, Hermitian projection and
+   trace renormalisation of every trial h; the lowest-sigma h is kept.  history (n_iter + 1 entries) receives
+   sigma_L1 at the start and after each accepted step; *n_history the count. */
+cy3q_status cy3q_lbfgs_refine(cy3q_solver* s, int32_t n_iter, int32_t m_history, double* history,
+                              int32_t* n_history);
+/* QuinticSolver::sigma_refine_lbfgs_with_restarts_gpu (quintic.rs:1100-1139): one run, then n_restarts runs
+   from the best h with a Hermitian uniform(-scale, scale) perturbation drawn from LCG(seed)
+   (perturb_h_block_hermitian, quintic.rs:1195-1223).  history (n_restarts + 1 entries) receives sigma after
+   each run; *best_sigma the lowest, whose h the handle keeps. */
+cy3q_status cy3q_lbfgs_refine_restarts(cy3q_solver* s, int32_t n_restarts, int32_t n_iter, int32_t m_history,
+                                       double perturb_scale, uint64_t seed, double* best_sigma, double* history);
 
 /* ---- Laplacian Galerkin spectrum + Yukawa overlap (templates: route34/metric_laplacian.rs:296-531,
         route34/yukawa_overlap_real.rs:298-372; the reference has no quintic version) ----

@@ -282,11 +282,21 @@ class OracleSolver:
                                  self.h_block.reshape(-1), C.byref(r))
         return r.value
 
-    def donaldson_solve(self, max_iter: int, tol: float) -> int:
-        """quintic.rs:433."""
+    def donaldson_step_unfixed(self) -> float:
+        """The reference's Donaldson step as it was before its 2026-04-29 fix (quintic.rs:1722-1726 describes
+        it): the trace-renormalised lower-index T(h) stored into h_block without inversion, residual
+        ||T(h) - h||_F.  Not the drop-in; kept only to reproduce run records made with it
+        (output/p5_3_multi_seed_ensemble.json)."""
+        t = t_operator(self.section_values, self.weights, self.h_block)
+        r = float(np.linalg.norm(t - self.h_block))
+        self.h_block = np.ascontiguousarray(t)
+        return r
+
+    def donaldson_solve(self, max_iter: int, tol: float, unfixed: bool = False) -> int:
+        """quintic.rs:433 (with `unfixed`, the earlier step of donaldson_step_unfixed)."""
         self.donaldson_residuals = []
         for _ in range(max_iter):
-            r = self.donaldson_step()
+            r = self.donaldson_step_unfixed() if unfixed else self.donaldson_step()
             self.donaldson_residuals.append(r)
             if r < tol:
                 break
@@ -352,6 +362,159 @@ class OracleSolver:
                                      self.n_basis, self.psi.real, self.psi.imag, self.h_block.reshape(-1), n_iter, lr,
                                      beta1, beta2, eps, hist)
         return list(hist[:done])
+
+
+def _unpack_h(hb: np.ndarray, n: int):
+    """h_block -> (h_re, h_im) (quintic.rs:4081-4085 packing)."""
+    return hb[0::2, 0::2].copy(), -hb[0::2, 1::2].copy()
+
+
+def _pack_renorm_h(hre: np.ndarray, him: np.ndarray, n: int) -> np.ndarray:
+    """pack_h_block_workspace + renormalise_h_trace_workspace (quintic.rs:2148-2160, 3169-3182)."""
+    hb = np.empty((2 * n, 2 * n))
+    hb[0::2, 0::2] = hre
+    hb[0::2, 1::2] = -him
+    hb[1::2, 0::2] = him
+    hb[1::2, 1::2] = hre
+    tr = 0.0
+    for a in range(n):
+        tr += hb[2 * a, 2 * a]
+    if tr > 1e-10:
+        hb *= n / tr
+    return hb
+
+
+def _apply_lbfgs_step(h_save: np.ndarray, d: np.ndarray, step: float, n: int) -> np.ndarray:
+    """apply_lbfgs_step (quintic.rs:2003-2047) from h_save."""
+    hre, him = _unpack_h(h_save, n)
+    nn = n * n
+    hre = hre + step * d[:nn].reshape(n, n)
+    iu = np.triu_indices(n, 1)
+    avg = 0.5 * (hre[iu] + hre.T[iu])
+    hre[iu] = avg
+    hre.T[iu] = avg
+    upd = step * d[nn:].reshape(n, n)[iu]
+    him[iu] += upd
+    him.T[iu] -= upd
+    him[np.diag_indices(n)] = 0.0
+    return _pack_renorm_h(hre, him, n)
+
+
+def _seq_dot(a: np.ndarray, b: np.ndarray) -> float:
+    return float(np.dot(a, b))
+
+
+def lbfgs_refine(solver, n_iter: int, m_history: int):
+    """QuinticSolver::sigma_refine_lbfgs_gpu_legacy (quintic.rs:678-890) on the oracle: the optimizer of the
+    reference step for step, the objective sigma_squared_and_gradient (quintic.rs:2714).  Returns the
+    sigma_L1 history (start and every accepted step) and leaves the lowest-sigma h in the solver."""
+    n = solver.n_basis
+    n_dof = 2 * n * n
+    f, g, sigma = solver.sigma_squared_and_gradient()
+    hist = []
+    if not np.isfinite(sigma):
+        return hist
+    hist.append(sigma)
+    best_sigma, best_h = sigma, solver.h_block.copy()
+    s_hist, y_hist, rho_hist = [], [], []
+    for _ in range(n_iter):
+        q = g.copy()
+        m = len(s_hist)
+        alphas = [0.0] * m
+        for k in range(m - 1, -1, -1):
+            a = rho_hist[k] * _seq_dot(s_hist[k], q)
+            alphas[k] = a
+            q -= a * y_hist[k]
+        gamma = 1.0
+        if m > 0:
+            sy, yy = rho_hist[-1], _seq_dot(y_hist[-1], y_hist[-1])
+            gamma = 1.0 / (sy * yy) if (yy > 1e-30 and np.isfinite(sy)) else 1.0
+        q *= gamma
+        for k in range(m):
+            b = rho_hist[k] * _seq_dot(y_hist[k], q)
+            q += s_hist[k] * (alphas[k] - b)
+        d = -q
+        gd = _seq_dot(g, d)
+        used = m > 0
+        if not np.isfinite(gd) or gd >= 0.0:
+            s_hist, y_hist, rho_hist = [], [], []
+            d = -g
+            gd = _seq_dot(g, d)
+            used = False
+            if gd >= 0.0:
+                break
+        gn = float(np.sqrt(_seq_dot(g, g)))
+        h_save = solver.h_block.copy()
+
+        def search(step0):
+            t = step0
+            for _ls in range(30):
+                solver.h_block = _apply_lbfgs_step(h_save, d, t, n)
+                ft, gt, st = solver.sigma_squared_and_gradient()
+                if np.isfinite(ft) and ft <= f + 1e-4 * t * gd:
+                    return t, ft, gt, st
+                t *= 0.5
+            return None
+
+        res = search(1.0 if used else (1.0 / gn if gn > 1e-30 else 1.0))
+        if res is None and used:
+            s_hist, y_hist, rho_hist = [], [], []
+            d = -g
+            gd = _seq_dot(g, d)
+            res = search(1.0 / gn if gn > 1e-30 else 1.0)
+        if res is None:
+            solver.h_block = h_save
+            break
+        step, f_new, g_new, s_new = res
+        sk, yk = step * d, g_new - g
+        sy = _seq_dot(sk, yk)
+        if sy > 1e-12:
+            s_hist.append(sk)
+            y_hist.append(yk)
+            rho_hist.append(1.0 / sy)
+            if len(s_hist) > m_history:
+                s_hist.pop(0)
+                y_hist.pop(0)
+                rho_hist.pop(0)
+        if np.isfinite(s_new) and s_new < best_sigma:
+            best_sigma, best_h = s_new, solver.h_block.copy()
+        f, g = f_new, g_new
+        hist.append(s_new)
+    solver.h_block = best_h
+    return hist
+
+
+def lbfgs_refine_restarts(solver, n_restarts: int, n_iter: int, m_history: int, perturb_scale: float, seed: int):
+    """QuinticSolver::sigma_refine_lbfgs_with_restarts_gpu (quintic.rs:1100-1139) on the oracle, with
+    perturb_h_block_hermitian (quintic.rs:1195-1223) drawing from LCG(seed)."""
+    n = solver.n_basis
+    lbfgs_refine(solver, n_iter, m_history)
+    best = solver.sigma()
+    best_h = solver.h_block.copy()
+    hist = [best]
+    u = lcg_uniforms(seed, n_restarts * n * n + 1)
+    pos = 0
+    for _ in range(n_restarts):
+        hre, him = _unpack_h(best_h, n)
+        for a in range(n):
+            hre[a, a] += perturb_scale * (u[pos] * 2.0 - 1.0)
+            pos += 1
+            for b in range(a + 1, n):
+                dr = perturb_scale * (u[pos] * 2.0 - 1.0)
+                di = perturb_scale * (u[pos + 1] * 2.0 - 1.0)
+                pos += 2
+                hre[a, b] += dr
+                hre[b, a] += dr
+                him[a, b] += di
+                him[b, a] -= di
+        solver.h_block = _pack_renorm_h(hre, him, n)
+        lbfgs_refine(solver, n_iter, m_history)
+        trial = solver.sigma()
+        hist.append(trial)
+        if np.isfinite(trial) and trial < best:
+            best, best_h = trial, solver.h_block.copy()
+    solver.h_block = best_h
+    return best, hist
 
 
 def laplacian_gram(F: np.ndarray, E: np.ndarray, c: np.ndarray):

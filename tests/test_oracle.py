@@ -202,3 +202,22 @@ def test_sigma_decreases_with_k(orc):  # quintic.rs:8603
         s.donaldson_solve(15, 1e-10)
         sig.append(s.sigma())
     assert sig[1] < sig[0]
+
+
+def test_lbfgs_refinement_oracle(orc):
+    """The oracle's restatement of the reference L-BFGS refinement (quintic.rs:678-890): sigma falls from the
+    balanced metric, every recorded value is finite, and the handle is left at the lowest sigma seen."""
+    o = orc.OracleSolver.new_with_sampler(2, 3000, 13, 1e-12, "sz")
+    o.donaldson_solve(10, 1e-10)
+    s0 = o.sigma()
+    hist = orc.lbfgs_refine(o, 6, 5)
+    assert len(hist) == 7 and all(np.isfinite(hist))
+    assert hist[0] == pytest.approx(s0, rel=1e-12)
+    assert min(hist) < 0.5 * s0
+    assert o.sigma() == pytest.approx(min(hist), rel=1e-12)
+    # restarts keep the best run
+    o2 = orc.OracleSolver.new_with_sampler(2, 3000, 13, 1e-12, "sz")
+    o2.donaldson_solve(10, 1e-10)
+    best, runs = orc.lbfgs_refine_restarts(o2, 2, 3, 5, 1e-3, 7)
+    assert len(runs) == 3 and best == min(runs)
+    assert o2.sigma() == pytest.approx(best, rel=1e-12)
