@@ -141,6 +141,25 @@ cy3q_status cy3q_lbfgs_refine(cy3q_solver* s, int32_t n_iter, int32_t m_history,
    each run; *best_sigma the lowest, whose h the handle keeps. */
 cy3q_status cy3q_lbfgs_refine_restarts(cy3q_solver* s, int32_t n_restarts, int32_t n_iter, int32_t m_history,
                                        double perturb_scale, uint64_t seed, double* best_sigma, double* history);
+/* Failure-detection hook, no reference counterpart: the handle's next split-precision balancing step starves
+   its own tensor-core issuer (the point-tile producer skips its first load), so a bounded device wait expires
+   after about 2 s, every role of the step's kernels winds down, and the step returns CY3Q_ERR_TIMEOUT with
+   the previous h kept.  No fault reaches the GPU and the handle steps normally afterwards.  Needs a
+   split-precision handle that has stepped once (CY3Q_ERR_UNSUPPORTED otherwise). */
+cy3q_status cy3q_debug_stall_next_step(cy3q_solver* s);
+
+/* ---- checkpoints and run manifest (no reference file format; the reference keeps this state in the public
+        fields of QuinticSolver, quintic.rs:117-165) ---- */
+/* Versioned checkpoint of the solve: h_block, Adam m, v and step count, and what identifies the problem (k,
+   basis, N, psi, seed, point count, precision, FS-Gram transform, FNV-1a hash of the points).  Written to a
+   temporary name and renamed, so an interrupted save leaves no partial file. */
+cy3q_status cy3q_checkpoint_save(const cy3q_solver* s, const char* path);
+/* Restores h_block and the Adam state into a handle holding the same points and basis; CY3Q_ERR_SHAPE when
+   the checkpoint belongs to another solve. */
+cy3q_status cy3q_checkpoint_load(cy3q_solver* s, const char* path);
+/* JSON description of the handle: library version, device, configuration, basis and sample sizes, h version,
+   launches, device bytes.  *needed receives the buffer size required (including the terminating zero). */
+cy3q_status cy3q_manifest(const cy3q_solver* s, char* buf, size_t len, size_t* needed);
 
 /* ---- Laplacian Galerkin spectrum + Yukawa overlap (templates: route34/metric_laplacian.rs:296-531,
         route34/yukawa_overlap_real.rs:298-372; the reference has no quintic version) ----

@@ -292,3 +292,29 @@ def test_lbfgs_refinement_split_precision(cy, orc):
     assert len(hm) == len(hf)
     np.testing.assert_allclose(hm, hf, rtol=1e-6)
     assert hm[-1] < hm[0]
+
+
+def test_checkpoint_resume_and_manifest(cy, orc, tmp_path):
+    """A checkpoint taken mid-solve (after balancing and an Adam refinement) restores h and the Adam state
+    into a fresh handle on the same points, whose next steps equal the original's bit for bit; a handle on
+    other points refuses it; the manifest describes the handle."""
+    o = _orc_set(orc, 3, 8000, 3, 0.5)
+    a = cy.QuinticSolver.from_points(3, o.points, o.weights, o.log_omega_sq, psi=0.5)
+    for _ in range(3):
+        a.donaldson_step()
+    a.sigma_refine_analytic(3, 1e-3)
+    path = str(tmp_path / "solve.ckp")
+    a.save_checkpoint(path)
+    b = cy.QuinticSolver.from_points(3, o.points, o.weights, o.log_omega_sq, psi=0.5)
+    b.load_checkpoint(path)
+    assert np.array_equal(a.h_block, b.h_block)
+    for _ in range(2):
+        assert a.donaldson_step() == b.donaldson_step()
+    assert np.array_equal(a.h_block, b.h_block)
+    other = cy.QuinticSolver.from_points(3, o.points[:7000], o.weights[:7000], o.log_omega_sq[:7000], psi=0.5)
+    with pytest.raises(cy.Cy3qError) as e:
+        other.load_checkpoint(path)
+    assert "ERR_SHAPE" in str(e.value)
+    man = a.manifest()
+    assert man["n_basis"] == 35 and man["n_points"] == 8000 and man["config"]["k"] == 3
+    assert man["adam_t"] == 3 and man["device"]["sm_count"] > 0 and man["config"]["precision"] == "fp64"

@@ -157,3 +157,31 @@ def test_config2_full_size_accuracy(cy):
     assert m.sigma() == pytest.approx(sf, rel=1e-6)
     f.close()
     m.close()
+
+
+def test_expired_device_wait_reports_timeout_and_recovers(cy, orc):
+    """Failure detection without a GPU fault: a step whose tensor-core issuer is starved (host hook, one step)
+    ends when its bounded wait expires, returns ERR_TIMEOUT and keeps the previous h; the next step runs
+    normally and equals a handle that took the same path (refactoring h) without the stall, bit for bit."""
+    import time
+
+    from papers_b200 import Cy3qError
+
+    o = orc.OracleSolver.new_with_psi_sz(3, 12000, 21, 0.5, reduced=True)
+    a = cy.QuinticSolver.from_points(3, o.points, o.weights, o.log_omega_sq, psi=0.5, reduced_basis=True,
+                                     precision="fp16x3")
+    b = cy.QuinticSolver.from_points(3, o.points, o.weights, o.log_omega_sq, psi=0.5, reduced_basis=True,
+                                     precision="fp16x3")
+    a.donaldson_step()
+    b.donaldson_step()
+    h1 = a.h_block
+    a.debug_stall_next_step()
+    t0 = time.perf_counter()
+    with pytest.raises(Cy3qError) as e:
+        a.donaldson_step()
+    assert "ERR_TIMEOUT" in str(e.value)
+    assert time.perf_counter() - t0 < 30.0
+    assert np.array_equal(a.h_block, h1)
+    b.h_block = b.h_block  # the same refactoring of h that the failed step leaves pending
+    assert a.donaldson_step() == b.donaldson_step()
+    assert np.array_equal(a.h_block, b.h_block)
