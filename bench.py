@@ -51,6 +51,10 @@ def parse():
     ap.add_argument("--adam-points", type=int, default=2_000_000, help="0 skips the sigma-Adam run")
     ap.add_argument("--adam-steps", type=int, default=200)
     ap.add_argument("--adam-minibatch", type=int, default=200_000)
+    ap.add_argument("--traffic-csv", default=None,
+                    help="ncu --page raw --csv export with dram__bytes_read.sum / dram__bytes_write.sum of the two "
+                         "tensor-core kernels; their per-point DRAM bytes replace the built-in figures")
+    ap.add_argument("--traffic-points", type=int, default=100096, help="padded points of the --traffic-csv capture")
     return ap.parse_args()
 
 
@@ -58,16 +62,39 @@ def parse():
 # clocks during the timed region
 # ------------------------------------------------------------------------------------------------
 class ClockSampler:
+    """SM clock and clock-event reasons of this process's GPU, sampled every 5 ms through NVML (the GPU found by
+    its UUID, so the index does not depend on CUDA_VISIBLE_DEVICES); nvidia-smi at 200 ms when NVML is not
+    available.  Reasons are kept when they were active in any sample."""
+
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
     def __init__(self, gpu_index: int):
         self.idx = gpu_index
         self.proc = None
+        self.nvml = None
         self.lines: list[str] = []
+        self.samples: list[tuple[float, int]] = []
+        self.smax = None
+        self._stop = threading.Event()
 
     def start(self):
+        try:
+            import pynvml
+            import torch
+
+            pynvml.nvmlInit()
+            uuid = "GPU-" + str(torch.cuda.get_device_properties(self.idx).uuid)
+            h = pynvml.nvmlDeviceGetHandleByUUID(uuid)
+            self.smax = float(pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM))
+            self.nvml = (pynvml, h)
+            self._t = threading.Thread(target=self._poll, daemon=True)
+            self._t.start()
+            return
+        except Exception:
+            self.nvml = None
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.FIELDS}",
                                           "--format=csv,noheader,nounits", "-lms", "200"],
@@ -77,11 +104,33 @@ class ClockSampler:
         except OSError:
             self.proc = None
 
+    def _poll(self):
+        pynvml, h = self.nvml
+        while not self._stop.is_set():
+            try:
+                self.samples.append((float(pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)),
+                                     int(pynvml.nvmlDeviceGetCurrentClocksEventReasons(h))))
+            except Exception:
+                pass
+            time.sleep(0.005)
+
     def _read(self):
         for line in self.proc.stdout:
             self.lines.append(line.strip())
 
     def stop(self) -> dict:
+        if self.nvml is not None:
+            self._stop.set()
+            self._t.join(timeout=5)
+            pynvml = self.nvml[0]
+            bits = {"hw_slowdown": pynvml.nvmlClocksEventReasonHwSlowdown,
+                    "hw_thermal_slowdown": pynvml.nvmlClocksEventReasonHwThermalSlowdown,
+                    "sw_thermal_slowdown": pynvml.nvmlClocksEventReasonSwThermalSlowdown,
+                    "sw_power_cap": pynvml.nvmlClocksEventReasonSwPowerCap}
+            sm = [c for c, _ in self.samples]
+            reasons = sorted({nm for _, r in self.samples for nm, bit in bits.items() if r & bit})
+            return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": self.smax, "reasons": reasons,
+                    "samples": len(sm), "source": "nvml, 5 ms"}
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.proc.terminate()
@@ -90,7 +139,6 @@ class ClockSampler:
         except subprocess.TimeoutExpired:
             self.proc.kill()
         sm, smax, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for ln in self.lines:
             parts = [p.strip() for p in ln.split(",")]
             if len(parts) < 9:
@@ -100,11 +148,11 @@ class ClockSampler:
                 smax = float(parts[2])
             except ValueError:
                 continue
-            for nm, v in zip(names, parts[5:9]):
+            for nm, v in zip(self.NAMES, parts[5:9]):
                 if v.lower().startswith("active"):
                     reasons.add(nm)
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "source": "nvidia-smi, 200 ms"}
 
 
 # ------------------------------------------------------------------------------------------------
@@ -138,6 +186,29 @@ def barrier(ws):
         import torch.distributed as dist
 
         dist.barrier()
+
+
+def traffic_from_csv(path, pts):
+    """Per-point DRAM bytes of umma_bergman_kernel / umma_gram_kernel from an ncu raw CSV export (ncu -i ...
+    --page raw --csv) of a capture over `pts` padded points."""
+    import csv
+
+    rows = list(csv.reader(open(path)))
+    hdr = rows[0]
+    try:
+        ik, ir, iw = hdr.index("Kernel Name"), hdr.index("dram__bytes_read.sum"), hdr.index("dram__bytes_write.sum")
+    except ValueError:
+        return None, None
+    unit = {"byte": 1.0, "Kbyte": 1e3, "Mbyte": 1e6, "Gbyte": 1e9}
+    u = rows[1]
+    out = {}
+    for r in rows[2:]:
+        for stage, name in (("bergman", "umma_bergman_kernel"), ("toperator", "umma_gram_kernel")):
+            if name in r[ik] and stage not in out:
+                out[stage] = (float(r[ir]) * unit.get(u[ir], 1.0) + float(r[iw]) * unit.get(u[iw], 1.0)) / pts
+    if len(out) != 2:
+        return None, None
+    return out, f"DRAM bytes per launch from {os.path.basename(path)} ({pts} points), scaled in points"
 
 
 def algorithmic(P, N):
@@ -430,26 +501,25 @@ def main():
     s.h_block = np.eye(2 * N)
 
     # ---- timed region: K balancing iterations, device-timed (the production path: each step's body is
-    # replayed from a CUDA graph) ----
+    # replayed from a CUDA graph).  The clock record is sampled every 5 ms from just before the timed
+    # region to its end (one 20-iteration solve at this workload takes about 25 ms) ----
     clk = ClockSampler(dev)
-    clk.start()
-    time.sleep(0.3)
     s.launch_count(reset=True)
     barrier(ws)
     torch.cuda.synchronize()
+    clk.start()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
     residuals = [s.donaldson_step() for _ in range(a.steps)]
     ev1.record(stream)
     torch.cuda.synchronize()
     barrier(ws)
-    ms = ev0.elapsed_time(ev1)
     clocks = clk.stop()
+    ms = ev0.elapsed_time(ev1)
     launches = s.launch_count(reset=True)
+    h_run = s.h_block
     ms_max = dist_max(ms, ws)
     value = ws * a.steps / (ms_max / 1e3)
-
-    h_run = s.h_block
 
     # ---- stage breakdown: the same K iterations again from h = I with per-stage CUDA events (eager
     # launches, so every stage boundary can be timed); gives the roofline kernel's launch duration ----
@@ -561,9 +631,14 @@ def main():
     stage_flops = {"toperator": alg["F_T"], "bergman": alg["F_K"]}
     stage_bytes = {"bergman": 2.0 * Pp * ldk * 4, "toperator": 1.0 * Pp * ldk * 4}
     # DRAM bytes per point of the two kernels (dram__bytes_read.sum + dram__bytes_write.sum of one ncu capture of
-    # each kernel on a 100,096-point case of this workload), scaled in points: both stream their operands once
-    traffic_per_point = {"bergman": (290.958848e6 + 136.252928e6) / 100096,
-                         "toperator": (183.617792e6 + 25.158656e6) / 100096}
+    # each kernel on the 100,096-point case of this workload, `--points 100000`), scaled in points: both stream
+    # their operands once.  --traffic-csv reads the figures from an ncu --page raw --csv export instead.
+    traffic_per_point, traffic_src = (traffic_from_csv(a.traffic_csv, a.traffic_points) if a.traffic_csv
+                                      else (None, None))
+    if traffic_per_point is None:
+        traffic_per_point = {"bergman": (307.214848e6 + 122.638336e6) / 100096,
+                             "toperator": (198.416896e6 + 8.093440e6) / 100096}
+        traffic_src = "DRAM bytes per launch scaled from the 100,096-point ncu capture of these kernels"
     cand = {k: v for k, v in stages.items() if k in stage_flops}
     dname, (dms, dcalls) = max(cand.items(), key=lambda kv: kv[1][0]) if cand else ("toperator", (ms, a.steps))
     avg_ms = dms / max(dcalls, 1)
@@ -593,7 +668,7 @@ def main():
     roof.update({"kernel_stage": dname, "avg_launch_ms": avg_ms,
                  "kernel": {"bergman": "umma_bergman_kernel", "toperator": "umma_gram_kernel"}[dname],
                  "algorithmic_flops_per_launch": stage_flops[dname],
-                 "traffic_note": "DRAM bytes per launch scaled from the 100k-point ncu capture",
+                 "traffic_note": traffic_src,
                  "stage_ms_per_step": {k: v[0] / max(v[1], 1) for k, v in stages.items()}})
 
     galerkin = None
