@@ -43,7 +43,10 @@ typedef enum {
   CY3Q_ERR_CANCELLED = 8,    /* request cancelled */
   CY3Q_ERR_UNSUPPORTED = 9,  /* option not supported by this build */
   CY3Q_ERR_NOT_PD = 10,      /* FS Gram matrix not positive-definite (quintic.rs:3148-3149) */
-  CY3Q_ERR_EMPTY = 11        /* no sample points (the reference constructors return None, quintic.rs:204) */
+  CY3Q_ERR_EMPTY = 11,       /* no sample points (the reference constructors return None, quintic.rs:204) */
+  CY3Q_ERR_MISS = 12,        /* no usable cached metric for the key (metric cache) */
+  CY3Q_ERR_STALE = 13        /* cached metric above the sigma quality threshold (MetricCacheError::StaleQuality,
+                                route34/metric_cache.rs:75-79) */
 } cy3q_status;
 
 typedef enum {
@@ -226,6 +229,7 @@ typedef struct {
   int32_t iterations;
   uint32_t n_basis;
   double submit_ms, start_ms, finish_ms;   /* times on the server clock */
+  int32_t cache_hit;         /* 1: h came from the server's metric cache and no iteration ran */
 } cy3q_result;
 typedef struct {
   uint64_t submitted, completed, failed, cancelled;
@@ -242,6 +246,11 @@ cy3q_status cy3q_cancel(cy3q_server* srv, uint64_t ticket);
 cy3q_status cy3q_server_stats_get(cy3q_server* srv, cy3q_server_stats* out);
 /* h of a completed request, [2N x 2N] in the reference packing. */
 cy3q_status cy3q_result_h(cy3q_server* srv, uint64_t ticket, double* h_block);
+/* Warm starts from the metric cache (below) under `root`, NULL or "" to turn them off: a submitted request
+   whose key (the request's fields with the server's sampler settings, max_iter = iterations, tol = 0) has a
+   cached metric completes at once with that h (cache_hit = 1, no device work); every request solved
+   afterwards is stored (by a writer thread, without the sample-cloud hash). */
+cy3q_status cy3q_server_set_cache(cy3q_server* srv, const char* root);
 
 /* ---- per-stage device timing (tracing; the reference's nearest analogue is
         AdamGradientKernel::compute_sigma_grad_h_only_profiled, gpu_adam.rs:1626-1767) ---- */
@@ -282,6 +291,39 @@ cy3q_status cy3q_sigma_noalloc(int32_t device, uint32_t k, int32_t reduced_basis
                                const double* d_points, const double* d_weights, const double* d_log_omega,
                                uint64_t n_points, const double* d_h_block, double* d_eta, double* sigma_l1,
                                void* cuda_stream);
+
+/* ---- content-addressed metric cache (route34/metric_cache.rs: ty_cache_path :175-193, load_or_solve_ty
+        :247-281, check_sigma_quality :318-340) ----
+   A balanced h_block is stored under a cache root in a file named by the key's readable fields and the first
+   16 hex digits of the SHA-256 of its canonical text:  quintic_k{k}_n{P}_i{max_iter}_seed{seed}_{hash}.cy3m.
+   The file holds the key text (checked on load, so a hash-prefix collision cannot alias), h_block, sigma_L1,
+   the last residual, the SHA-256 of the sample cloud (points, weights, log|Omega|^2) and a SHA-256 of the
+   whole file; it is written to a temporary name and renamed. */
+typedef struct {
+  uint32_t k;
+  double psi_re, psi_im;
+  uint64_t n_points;         /* requested points */
+  uint64_t seed;
+  int32_t sampler, fermat_variant, dk_iters, newton_polish, reduced_basis, precision;  /* as in cy3q_config */
+  int32_t max_iter;          /* iteration cap of the solve */
+  double tol;                /* its residual tolerance (0: a fixed iteration count) */
+} cy3q_cache_key;
+#define CY3Q_SIGMA_QUALITY_THRESHOLD 1.0e-3   /* SIGMA_QUALITY_THRESHOLD, route34/metric_cache.rs:65 */
+/* The key of a handle's configuration (TyKeyMaterial, metric_cache.rs:131-142, for the quintic). */
+cy3q_status cy3q_cache_key_of(const cy3q_solver* s, int32_t max_iter, double tol, cy3q_cache_key* key);
+/* The cache file path of `key` under `root` (ty_cache_path); no device work, no file access. */
+cy3q_status cy3q_cache_path(const char* root, const cy3q_cache_key* key, char* path, size_t len);
+/* Stores the handle's h_block with sigma_l1 and residual (NaN allowed) and its sample-cloud hash. */
+cy3q_status cy3q_cache_store(const char* root, const cy3q_cache_key* key, cy3q_solver* s, double sigma_l1,
+                             double residual);
+/* Hit: installs the cached h_block in the handle and returns OK with sigma_l1 and residual (either may be
+   NULL).  CY3Q_ERR_MISS when there is no file, it is damaged, it belongs to another key or basis size, or the
+   handle holds points whose cloud hash differs; with strict != 0, CY3Q_ERR_STALE when the cached sigma is not
+   below CY3Q_SIGMA_QUALITY_THRESHOLD (the handle's h is then unchanged). */
+cy3q_status cy3q_cache_load(const char* root, const cy3q_cache_key* key, cy3q_solver* s, int32_t strict,
+                            double* sigma_l1, double* residual);
+/* SHA-256 (FIPS 180-4) of n bytes as 64 hex digits and a terminating zero (hex65 holds 65 bytes). */
+cy3q_status cy3q_sha256_hex(const void* data, uint64_t n, char* hex65);
 
 /* ---- build / device information ---- */
 const char* cy3q_version(void);
