@@ -85,13 +85,15 @@ def test_mixed_fs_gram_kat(cy, orc):
     assert m.sigma() == pytest.approx(rec["sigma_donaldson"], rel=1e-6)
 
 
-# ---- sigma pass on the int8 tensor cores (Y = X . h with four 7-bit digits, exact int32 accumulation) ----
-# At a fixed h the split sigma pass must agree with the FP64 pass: sigma_L1 within 2e-8 relative,
-# sigma_L2^2 (a mean of squared deviations) within 5e-8, eta per point within 1e-6 relative (the
-# per-point metric carries ~2e-8 relative error at the worst points), the gradient of sigma_L2^2
-# within 1e-6 relative Frobenius.
+# ---- sigma on the tensor cores at a fixed h, against the FP64 pass ----
+# sigma() of a split-precision handle runs the sigma forms kernel (the six section rows of each point
+# times the factor R = pack(L^{-1}) of h in fp16x3, the 21 forms as Gram entries of L^{-1} x, FP64 metric
+# algebra) for bases up to 330 sections: sigma_L1 within 1e-6 relative (the north star's bar; measured
+# 1e-8 .. 2.5e-7 for k = 3 .. 6), eta per point within 5e-6.  Larger bases (k = 8) and the gradient use
+# the int8 digit pass (Y = X . h with four 7-bit digits, exact int32 accumulation): sigma_L1 within 2e-8,
+# sigma_L2^2 within 5e-8, eta within 1e-6, the gradient of sigma_L2^2 within 1e-6 relative Frobenius.
 @pytest.mark.parametrize("k,psi,reduced,P", [(4, 0.5, False, 30000), (6, 0.1 + 0.2j, True, 40000),
-                                             (8, 0.1 + 0.2j, True, 12000)])
+                                             (7, 0.3, True, 20000), (8, 0.1 + 0.2j, True, 12000)])
 def test_tensor_sigma_pass_matches_fp64(cy, orc, k, psi, reduced, P):
     g = cy.QuinticSolver(k, P, 17, psi, reduced_basis=reduced)
     for _ in range(3):
@@ -100,13 +102,17 @@ def test_tensor_sigma_pass_matches_fp64(cy, orc, k, psi, reduced, P):
     eta64 = g.eta()
     l2_64, gr64, _ = g.sigma_squared_and_gradient()
     g.set_precision("fp16x3")
+    forms = g.n_basis <= 330
     s16 = g.sigma()
     eta16 = g.eta()
-    l2_16, gr16, _ = g.sigma_squared_and_gradient()
-    assert abs(s16 / s64 - 1) <= 2e-8
     m = np.isfinite(eta64)
     assert np.array_equal(m, np.isfinite(eta16))
-    assert np.max(np.abs(eta16[m] / eta64[m] - 1)) <= 1e-6
+    assert abs(s16 / s64 - 1) <= (1e-6 if forms else 2e-8)
+    assert np.max(np.abs(eta16[m] / eta64[m] - 1)) <= (5e-6 if forms else 1e-6)
+    l2_16, gr16, l1_16 = g.sigma_squared_and_gradient()
+    eta8 = g.eta()
+    assert abs(l1_16 / s64 - 1) <= 2e-8
+    assert np.max(np.abs(eta8[m] / eta64[m] - 1)) <= 1e-6
     assert abs(l2_16 / l2_64 - 1) <= 5e-8
     assert relf(gr16, gr64) <= 1e-6
 
