@@ -27,9 +27,8 @@ _ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
 
 def build(force: bool = False) -> str:
     """Compile liboracle.so with the committed Makefile (gcc, -ffp-contract=off)."""
-    if force or not os.path.exists(_LIB_PATH) or os.path.getmtime(_LIB_PATH) < os.path.getmtime(
-        os.path.join(_HERE, "cy3_oracle.cpp")
-    ):
+    srcs = [os.path.join(_HERE, f) for f in ("cy3_oracle.cpp", "ty_oracle.cpp", "Makefile")]
+    if force or not os.path.exists(_LIB_PATH) or os.path.getmtime(_LIB_PATH) < max(map(os.path.getmtime, srcs)):
         subprocess.check_call(["make", "-s", "-C", _HERE, "liboracle.so"])
     return _LIB_PATH
 
@@ -83,6 +82,25 @@ def lib():
     L.orc_laplacian_gram.restype = d
     L.orc_yukawa.argtypes = [_dp, _dp, sz, d, d, C.c_int, _dp, C.c_int, _dp]
     L.orc_yukawa.restype = C.c_int
+    vp = C.c_void_p
+    L.orc_ty_rng_u64.argtypes = [C.c_uint64, sz, vp]
+    L.orc_ty_normals.argtypes = [C.c_uint64, sz, _dp]
+    L.orc_ty_sample.argtypes = [C.c_uint64, sz, C.c_int, C.c_int, _dp, _dp, _dp, _ip]
+    L.orc_ty_sample.restype = sz
+    L.orc_ty_post_process.argtypes = [_dp, _dp, _dp, _dp, _ip]
+    L.orc_ty_post_process.restype = C.c_int
+    L.orc_ty_groebner_lms.argtypes = [_ip, C.c_int]
+    L.orc_ty_groebner_lms.restype = C.c_int
+    L.orc_ty_basis.argtypes = [C.c_int, _ip, C.c_int]
+    L.orc_ty_basis.restype = C.c_int
+    L.orc_ty_sections.argtypes = [_dp, sz, _ip, C.c_int, _dp, vp]
+    L.orc_ty_frames.argtypes = [_dp, _ip, sz, _dp]
+    L.orc_ty_donaldson_step.argtypes = [_dp, _dp, sz, C.c_int, _dp, _dp, d]
+    L.orc_ty_donaldson_step.restype = d
+    L.orc_ty_sigma.argtypes = [_dp, _dp, _dp, sz, C.c_int, _dp, _dp, vp]
+    L.orc_ty_sigma.restype = d
+    L.orc_ty_solve.argtypes = [C.c_int, sz, C.c_int, d, C.c_uint64, _dp, _dp, _dp, C.c_int, vp, vp, sz]
+    L.orc_ty_solve.restype = C.c_int
     _lib = L
     return L
 
@@ -539,3 +557,122 @@ def laplacian_eigs(M: np.ndarray, K: np.ndarray, n_eigs: int = 40, reg: float = 
     Mr = M + reg * np.linalg.norm(M) * np.eye(n)
     ev = scipy.linalg.eigh(K, Mr, eigvals_only=True)
     return np.sort(np.abs(ev))[:n_eigs]
+
+
+# ---------------------------------------------------------------------------------------------
+# Tian-Yau (oracle/ty_oracle.cpp): the reference's solve_ty_metric path (route34/ty_metric.rs)
+# ---------------------------------------------------------------------------------------------
+def ty_rng_u64(seed: int, n: int) -> np.ndarray:
+    """First n u64 of ChaCha8Rng::seed_from_u64(seed) (rand_chacha 0.9)."""
+    out = np.empty(n, dtype=np.uint64)
+    lib().orc_ty_rng_u64(int(seed), int(n), out.ctypes.data)
+    return out
+
+
+def ty_normals(seed: int, n: int) -> np.ndarray:
+    """First n StandardNormal draws (rand_distr 0.5 ziggurat) from ChaCha8Rng::seed_from_u64(seed)."""
+    out = np.empty(n)
+    lib().orc_ty_normals(int(seed), int(n), out)
+    return out
+
+
+def ty_sample(n: int, seed: int, gpu_stream: bool = False, z3: bool = True):
+    """CicySampler::sample_batch (cicy_sampler.rs:600) [+ apply_z3_quotient].  gpu_stream draws the
+    line inputs as sample_batch_gpu does (max(4n, 64) lines, one Newton attempt each).
+    Returns (coords [P,16], omega [P] complex, weight [P], zw [P,2])."""
+    coords = np.empty((n, 16))
+    om = np.empty((n, 2))
+    w = np.empty(n)
+    zw = np.empty((n, 2), dtype=np.int32)
+    P = lib().orc_ty_sample(int(seed), int(n), int(gpu_stream), int(z3), coords, om, w, zw)
+    return coords[:P].copy(), (om[:P, 0] + 1j * om[:P, 1]), w[:P].copy(), zw[:P].copy()
+
+
+def ty_post_process(x: np.ndarray):
+    """post_process_solved_point (cicy_sampler.rs:452) of one line solution x [16]; None on rejection."""
+    coords = np.empty((1, 16))
+    om = np.empty((1, 2))
+    w = np.empty(1)
+    zw = np.empty((1, 2), dtype=np.int32)
+    if not lib().orc_ty_post_process(np.ascontiguousarray(x, dtype=np.float64), coords, om, w, zw):
+        return None
+    return coords[0], complex(om[0, 0], om[0, 1]), float(w[0]), zw[0]
+
+
+def ty_groebner_lms() -> np.ndarray:
+    """Leading monomials of the reduced deg-lex Groebner basis of the Tian-Yau ideal (groebner.rs:556)."""
+    out = np.zeros(4096 * 8, dtype=np.int32)
+    n = lib().orc_ty_groebner_lms(out, 4096)
+    return out[: n * 8].reshape(n, 8)
+
+
+def ty_basis(k: int) -> np.ndarray:
+    """build_ty_invariant_reduced_basis (ty_metric.rs:870): [N, 8] exponents."""
+    cap = 20000
+    out = np.zeros(cap * 8, dtype=np.int32)
+    n = lib().orc_ty_basis(int(k), out, cap)
+    return out[: n * 8].reshape(n, 8)
+
+
+def ty_sections(coords: np.ndarray, basis: np.ndarray, derivs: bool = True):
+    """Section values [P, 2N] and derivatives [P, 8, 2N] (ty_metric.rs:930-1000)."""
+    coords = np.ascontiguousarray(coords, dtype=np.float64)
+    basis = np.ascontiguousarray(basis, dtype=np.int32)
+    P, N = coords.shape[0], basis.shape[0]
+    vals = np.empty((P, 2 * N))
+    ders = np.empty((P, 8, 2 * N)) if derivs else None
+    lib().orc_ty_sections(coords, P, basis, N, vals, ders.ctypes.data if derivs else None)
+    return (vals, ders) if derivs else vals
+
+
+def ty_frames(coords: np.ndarray, zw: np.ndarray) -> np.ndarray:
+    """ty_affine_chart_frame (ty_metric.rs:1929) per point: [P, 3, 8] complex."""
+    coords = np.ascontiguousarray(coords, dtype=np.float64)
+    P = coords.shape[0]
+    out = np.empty((P, 3, 16))
+    lib().orc_ty_frames(coords, np.ascontiguousarray(zw, dtype=np.int32), P, out)
+    return out[..., 0::2] + 1j * out[..., 1::2]
+
+
+def ty_donaldson_step(vals: np.ndarray, w: np.ndarray, h: np.ndarray, alpha: float = 1.0):
+    """donaldson_iteration (ty_metric.rs:1062): h (N x N complex, upper index) -> (h_new, residual)."""
+    P, N = vals.shape[0], vals.shape[1] // 2
+    hr = np.ascontiguousarray(h.real, dtype=np.float64).copy()
+    hi = np.ascontiguousarray(h.imag, dtype=np.float64).copy()
+    r = lib().orc_ty_donaldson_step(np.ascontiguousarray(vals), np.ascontiguousarray(w, dtype=np.float64),
+                                    P, N, hr, hi, float(alpha))
+    return hr + 1j * hi, r
+
+
+def ty_sigma(coords: np.ndarray, omega_sq: np.ndarray, w: np.ndarray, k: int, h: np.ndarray):
+    """compute_sigma (ty_metric.rs:1402) on the points for metric h: (sigma, eta [P])."""
+    coords = np.ascontiguousarray(coords, dtype=np.float64)
+    P = coords.shape[0]
+    eta = np.empty(P)
+    s = lib().orc_ty_sigma(coords, np.ascontiguousarray(omega_sq, dtype=np.float64),
+                           np.ascontiguousarray(w, dtype=np.float64), P, int(k),
+                           np.ascontiguousarray(h.real, dtype=np.float64),
+                           np.ascontiguousarray(h.imag, dtype=np.float64), eta.ctypes.data)
+    return s, eta
+
+
+def ty_solve(k: int, n_sample: int, max_iter: int, tol: float, seed: int):
+    """solve_ty_metric (ty_metric.rs:461) with the spec defaults of cy3_metric_unified.rs:249-261.
+    Returns a dict with n_points, n_basis, iterations_run, sigma_fs_identity, sigma_final,
+    final_donaldson_residual, sigma_history, donaldson_history and h (N x N complex)."""
+    rec = np.zeros(6)
+    cap = max(8, 8 * max_iter + 8)
+    sh = np.zeros(cap)
+    rh = np.zeros(cap)
+    hcap = 4096 * 4096
+    n_est = int(ty_basis(k).shape[0])
+    hr = np.zeros(n_est * n_est)
+    hi = np.zeros(n_est * n_est)
+    n = lib().orc_ty_solve(int(k), int(n_sample), int(max_iter), float(tol), int(seed), rec, sh, rh, cap,
+                           hr.ctypes.data, hi.ctypes.data, hr.size)
+    if n < 0:
+        raise RuntimeError(f"orc_ty_solve failed ({n})")
+    N = int(rec[1])
+    return dict(n_points=int(rec[0]), n_basis=N, iterations_run=int(rec[2]), sigma_fs_identity=rec[3],
+                sigma_final=rec[4], final_donaldson_residual=rec[5], sigma_history=sh[:n].copy(),
+                donaldson_history=rh[:n].copy(), h=(hr + 1j * hi).reshape(N, N))

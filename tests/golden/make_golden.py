@@ -15,8 +15,14 @@ use next to this script; the fixtures are committed, so the tests never read the
   fixed its Donaldson step (they store T(h) without inverting it, quintic.rs:1722-1726), so the Donaldson
   and refinement values pin the oracle's restatement of that earlier step and, through it, the analytic
   sigma gradient and the Adam update; sigma at h = I does not depend on the step.
+* p5_10_ty_schoen_5sigma.json, bit_exact_fix/p5_10_xoshiro_reduced.json and
+  ../tests/data/p5_10_determinism_golden.json -> ty_kat.json: the Tian-Yau records of the reference's
+  solve_ty_metric (src/route34/ty_metric.rs:461; spec of src/route34/cy3_metric_unified.rs:242-261): k = 3,
+  20 seeds at n = 40,000 and 3 seeds at n = 2,000 (100 and 30 iterations, tolerance 1e-6), and the
+  determinism record at n = 200 (5 iterations; bit patterns decoded to floats).
 """
 import json
+import struct
 import os
 import sys
 
@@ -65,8 +71,45 @@ def p5_3(src_dir):
     return "p5_3_kat.json", out
 
 
+def ty(src_dir):
+    out = {
+        "source": ["substrate_sm_derivation/cy3_solver/output/p5_10_ty_schoen_5sigma.json",
+                   "substrate_sm_derivation/cy3_solver/output/bit_exact_fix/p5_10_xoshiro_reduced.json",
+                   "substrate_sm_derivation/cy3_solver/tests/data/p5_10_determinism_golden.json"],
+        "protocol": "TianYauSolver.solve_metric(Cy3MetricSpec::TianYau { k, n_sample, max_iter, donaldson_tol, seed }): "
+                    "CicySampler::sample_batch + Z/3 quotient, invariant Groebner-reduced basis, h = I, "
+                    "donaldson_iteration until residual < tol, sigma after every iteration",
+        "records": [],
+    }
+    for name, max_iter in (("p5_10_ty_schoen_5sigma.json", None), (os.path.join("bit_exact_fix", "p5_10_xoshiro_reduced.json"), 30)):
+        ref = json.load(open(os.path.join(src_dir, name)))
+        for cand in ref["candidates"]:
+            if cand["candidate"] != "TY":
+                continue
+            for rec in cand["per_seed"]:
+                out["records"].append({
+                    "k": rec["k"], "n_pts": ref["n_pts"], "seed": rec["seed"],
+                    "max_iter": max_iter or ref["donaldson_iters"], "tol": ref["donaldson_tol"],
+                    "n_basis": rec["n_basis"], "iterations_run": rec["iterations_run"],
+                    "sigma_fs_identity": rec["sigma_fs_identity"], "sigma_final": rec["sigma_final"],
+                    "final_donaldson_residual": rec["final_donaldson_residual"],
+                })
+    gold = json.load(open(os.path.join(src_dir, os.pardir, "tests", "data", "p5_10_determinism_golden.json")))
+    f64 = lambda b: struct.unpack("<d", struct.pack("<Q", b))[0]
+    for rec in gold["records"]:
+        if rec["candidate"] != "TY":
+            continue
+        out["records"].append({
+            "k": rec["k"], "n_pts": rec["n_pts"], "seed": rec["seed"], "max_iter": rec["donaldson_iters"],
+            "tol": rec["donaldson_tol"], "n_basis": rec["n_basis"], "iterations_run": rec["iterations_run"],
+            "sigma_fs_identity": f64(rec["sigma_fs_identity_bits"]), "sigma_final": f64(rec["sigma_final_bits"]),
+            "final_donaldson_residual": f64(rec["final_donaldson_residual_bits"]),
+        })
+    return "ty_kat.json", out
+
+
 def main(src_dir):
-    for make in (p5_9, p5_3):
+    for make in (p5_9, p5_3, ty):
         name, out = make(src_dir)
         dst = os.path.join(HERE, name)
         json.dump(out, open(dst, "w"), indent=1)
