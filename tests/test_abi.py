@@ -9,7 +9,8 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
 def _declared():
-    src = open(os.path.join(ROOT, "include", "cy3q.h")).read()
+    inc = os.path.join(ROOT, "include")
+    src = "".join(open(os.path.join(inc, f)).read() for f in sorted(os.listdir(inc)) if f.endswith(".h"))
     src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
     return sorted(set(re.findall(r"\b(cy3q_[a-z0-9_]+)\s*\(", src)))
 
@@ -32,9 +33,9 @@ def test_library_exports_every_declared_symbol(L):
 
 
 def test_python_binding_covers_header(L):
-    from papers_b200 import cy3q
+    from papers_b200 import cy3q, ty
 
-    assert sorted(cy3q.EXPORTS) == _declared()
+    assert sorted(cy3q.EXPORTS + ty.TY_EXPORTS) == _declared()
 
 
 def test_no_cpu_fallback_without_gpu(L):
