@@ -50,7 +50,7 @@ def parse():
     ap.add_argument("--galerkin-points", type=int, default=1_000_000, help="0 skips the Laplacian / Yukawa run")
     ap.add_argument("--adam-points", type=int, default=2_000_000, help="0 skips the sigma-Adam run")
     ap.add_argument("--adam-steps", type=int, default=200)
-    ap.add_argument("--ty-points", type=int, default=40_000, help="0 skips the Tian-Yau solve")
+    ap.add_argument("--ty-points", type=int, default=40_000, help="0 skips the Tian-Yau and Schoen solves")
     ap.add_argument("--adam-minibatch", type=int, default=200_000)
     ap.add_argument("--traffic-csv", default=None,
                     help="ncu --page raw --csv export with dram__bytes_read.sum / dram__bytes_write.sum of the two "
@@ -420,20 +420,17 @@ def adam_run(a, dev, stream):
             "stage_ms_per_call": stages}
 
 
-def ty_run(a, dev, cpu: bool):
-    """Tian-Yau solve_ty_metric at the reference's production setting (k = 3, 40,000 points, up to 100
-    iterations to 1e-6, sigma after every iteration) through the public API: the device sampler, the balancing
-    loop and the sigma passes, wall-clock around the call (it synchronises every iteration, as the reference's
-    loop reads each residual).  The CPU side times the oracle's port on the same cloud for two full iterations
-    (Donaldson + sigma, all host threads); the reference's own record for this setting is 20.1 s per seed."""
+def cicy_run(a, dev, cfg, warm_cfg, basis, sigma_fn, cpu: bool, record_s: float):
+    """One complete-intersection solve (solve_ty_metric / solve_schoen_metric) at the reference's production
+    setting through the public API: the device sampler, the balancing loop and the sigma passes, wall-clock
+    around the call (it synchronises every iteration, as the reference's loop reads each residual).  The CPU
+    side times the oracle's port on the same cloud for two full iterations (Donaldson + sigma, all host
+    threads); `record_s` is the reference's own recorded time per seed for this setting."""
     import torch
 
     from papers_b200 import ty
 
-    cfg = ty.TyMetricConfig(k_degree=3, n_sample=a.ty_points, max_iter=100, donaldson_tol=1e-6, seed=a.seed,
-                            device=dev)
-    ty.solve_ty_metric(ty.TyMetricConfig(k_degree=3, n_sample=2000, max_iter=3, donaldson_tol=1e-6,
-                                         seed=a.seed, device=dev))  # warm: library kernels and cuSOLVER loaded
+    ty.solve_ty_metric(warm_cfg)  # warm: library kernels and cuSOLVER loaded
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     r = ty.solve_ty_metric(cfg)
@@ -452,26 +449,48 @@ def ty_run(a, dev, cpu: bool):
     for _ in range(5):
         ws.sigma()
     sigma_ms = 1e3 * (time.perf_counter() - t0) / 5
-    out = {"workload": f"Tian-Yau k=3 N={r['n_basis']}, {n} pts, tol 1e-6", "solve_s": solve_s,
-           "iterations": r["iterations_run"], "sigma_final": r["sigma_final"],
+    out = {"workload": f"N={r['n_basis']}, {n} pts, tol {cfg.donaldson_tol:g}", "solve_s": solve_s,
+           "reference_record_s": record_s, "iterations": r["iterations_run"], "sigma_final": r["sigma_final"],
            "sigma_fs_identity": r["sigma_fs_identity"], "residual": r["final_donaldson_residual"],
-           "sample_ms": sample_ms, "step_ms": step_ms, "sigma_ms": sigma_ms}
+           "sample_ms": sample_ms, "step_ms": step_ms, "sigma_ms": sigma_ms,
+           "gpu_ms_per_iteration": step_ms + sigma_ms}
     if cpu:
         import oracle
 
         oracle.set_threads(os.cpu_count() or 1)
         c, o2, w = ws.points()
-        vals = oracle.ty_sections(c, oracle.ty_basis(3), derivs=False)
+        vals = oracle.ty_sections(c, basis, derivs=False)
         h = np.eye(r["n_basis"], dtype=complex)
         t0 = time.perf_counter()
         for _ in range(2):
             h, _res = oracle.ty_donaldson_step(vals, w, h)
-            oracle.ty_sigma(c, o2, w, 3, h)
+            sigma_fn(c, o2, w, h)
         cpu_iter_s = (time.perf_counter() - t0) / 2
         out.update({"cpu_s_per_iteration": cpu_iter_s, "cpu_threads": oracle.threads(),
-                    "gpu_ms_per_iteration": step_ms + sigma_ms,
                     "speedup_per_iteration": 1e3 * cpu_iter_s / (step_ms + sigma_ms)})
     ws.close()
+    return out
+
+
+def ty_run(a, dev, cpu: bool):
+    """Tian-Yau k = 3 and Schoen (3, 3, 1) at 40,000 points, up to 100 iterations to 1e-6 (the reference's
+    P5.10 production setting; its records: 20.1 s and 3.8 s per seed for seed 42)."""
+    from papers_b200 import ty
+
+    out = {}
+    tyb = scb = None
+    if cpu:  # the CPU columns time the oracle's port; the GPU columns do not use it
+        import oracle
+
+        tyb, scb = oracle.ty_basis(3), oracle.schoen_basis(3, 3, 1)
+    cfg = ty.TyMetricConfig(k_degree=3, n_sample=a.ty_points, max_iter=100, donaldson_tol=1e-6, seed=a.seed, device=dev)
+    warm = ty.TyMetricConfig(k_degree=3, n_sample=2000, max_iter=3, donaldson_tol=1e-6, seed=a.seed, device=dev)
+    out["tian_yau"] = cicy_run(a, dev, cfg, warm, tyb,
+                               lambda c, o2, w, h: __import__("oracle").ty_sigma(c, o2, w, 3, h), cpu, 20.11)
+    scfg = ty.SchoenMetricConfig(n_sample=a.ty_points, max_iter=100, donaldson_tol=1e-6, seed=a.seed, device=dev)
+    swarm = ty.SchoenMetricConfig(n_sample=2000, max_iter=3, donaldson_tol=1e-6, seed=a.seed, device=dev)
+    out["schoen"] = cicy_run(a, dev, scfg, swarm, scb,
+                             lambda c, o2, w, h: __import__("oracle").schoen_sigma(c, o2, w, (3, 3, 1), h), cpu, 3.77)
     return out
 
 
@@ -766,7 +785,7 @@ def main():
         # stdout keeps scalars, so that it stays short and the accuracy figures sit at its end
         detail = {"stage_ms_per_step": roof.pop("stage_ms_per_step", None), "hbm_view": roof.pop("hbm_view", None),
                   "tensor_view": roof.pop("tensor_view", None), "sigma_stage_ms": sigma_stages,
-                  "laplacian": galerkin, "sigma_adam": adam, "serving": serving, "tian_yau": tian_yau}
+                  "laplacian": galerkin, "sigma_adam": adam, "serving": serving, "cicy": tian_yau}
         print("bench detail: " + json.dumps(detail), file=sys.stderr, flush=True)
 
         def pick(d, keys):
@@ -787,8 +806,12 @@ def main():
                                        ["sigma_l1_rel_err", "grad_rel_frobenius"]) if adam else None,
                 "serving": pick(serving, ["error", "failed", "p50_ms", "p99_ms", "iters_per_s",
                                           "fp64_one_at_a_time_iters_per_s"]),
-                "tian_yau": pick(tian_yau, ["error", "solve_s", "iterations", "sigma_final", "gpu_ms_per_iteration",
-                                            "cpu_s_per_iteration"]),
+                "tian_yau": pick((tian_yau or {}).get("tian_yau", tian_yau),
+                                 ["error", "solve_s", "iterations", "sigma_final", "gpu_ms_per_iteration",
+                                  "cpu_s_per_iteration"]) if tian_yau else None,
+                "schoen": pick((tian_yau or {}).get("schoen"), ["solve_s", "iterations", "sigma_final",
+                                                               "gpu_ms_per_iteration", "cpu_s_per_iteration"])
+                if tian_yau and "schoen" in tian_yau else None,
                 "residual_last": residuals[-1], "sigma": sig,
                 "sigma_evals_per_s": sigma_per_s, "sigma_evals_per_s_fp64": sigma64_per_s,
                 "fp64_iters_per_s": fp64_per_s, "speedup_vs_fp64": (value / fp64_per_s) if fp64_per_s else None,

@@ -17,6 +17,8 @@
  *   h_re, h_im [N x N] f64 row-major: the upper-index metric G = h_re + i h_im of ty_metric.rs:404-424
  *
  * Host memory in and out, device state owned by the handle; status codes of cy3q.h; one thread per handle.
+ * A handle holds one complete-intersection solve: Tian-Yau (cy3q_ty_create) or Schoen (cy3q_schoen_create,
+ * at the end of this header).
  */
 #ifndef CY3Q_TY_H
 #define CY3Q_TY_H
@@ -83,6 +85,36 @@ cy3q_status cy3q_ty_sigma(cy3q_ty* t, double* sigma, double* eta, long long cap)
 cy3q_status cy3q_ty_solve(cy3q_ty* t, cy3q_ty_result* out, double* sigma_hist, double* res_hist, int hist_cap);
 /* Kernel launches made by the handle so far. */
 cy3q_status cy3q_ty_launch_count(const cy3q_ty* t, uint64_t* n);
+
+/*
+ * Schoen: the Z/3 x Z/3 quotient of the complete intersection in CP^2 x CP^2 x CP^1 with coordinates
+ * x_0..x_2, y_0..y_2, t_0, t_1 (the coords layout above in this order),
+ *     F1 = (x0^3 + x1^3 + x2^3) t0 + x0 x1 x2 t1,   F2 = (y0^3 + y1^3 + y2^3) t1 + y0 y1 y2 t0
+ * (`SchoenPoly::z3xz3_invariant_default`, src/route34/schoen_sampler.rs:188-216), solved by
+ * `solve_schoen_metric` (src/route34/schoen_metric.rs:766-1000) through the same handle type and entry points
+ * (cy3q_ty_sample, _set_points, _donaldson_step, _sigma, _solve, _get_h ...).  The sampler draws one Newton
+ * attempt per line (origin, two directions, t: 52 draws) and keeps the first n accepted lines; the weights are
+ * normalised by the inverse of their sum and multiplied by 1/9 (schoen_sampler.rs:555-560, 1177-1185).
+ */
+typedef struct {
+  int d_x, d_y, d_t;          /* tri-degree of the section basis (SchoenMetricConfig::d_x, d_y, d_t) */
+  long long n_sample;
+  int max_iter;
+  double donaldson_tol;
+  uint64_t seed;
+  int apply_z3xz3_quotient;   /* divide the weights by 9 (SchoenMetricConfig::apply_z3xz3_quotient) */
+  double damping;             /* <= 0: the reference's rule (static 1, adaptive when d_x + d_y + d_t >= 10,
+                                 schoen_metric.rs:649-665); otherwise a static alpha */
+  int sigma_every_iter;
+  int device;
+} cy3q_schoen_config;
+
+/* SchoenMetricConfig defaults with the Cy3MetricSpec::Schoen overrides (cy3_metric_unified.rs:289-320). */
+cy3q_status cy3q_schoen_config_default(cy3q_schoen_config* cfg);
+/* build_schoen_invariant_reduced_basis (schoen_metric.rs:1185): Gamma-invariant tri-degree monomials not in
+   the leading-monomial ideal of the reduced deg-lex Groebner basis of schoen_generators (groebner.rs:705). */
+cy3q_status cy3q_schoen_basis(int d_x, int d_y, int d_t, int* n, int* exps, int cap);
+cy3q_status cy3q_schoen_create(const cy3q_schoen_config* cfg, cy3q_ty** out);
 
 #ifdef __cplusplus
 }

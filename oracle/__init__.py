@@ -27,7 +27,7 @@ _ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
 
 def build(force: bool = False) -> str:
     """Compile liboracle.so with the committed Makefile (gcc, -ffp-contract=off)."""
-    srcs = [os.path.join(_HERE, f) for f in ("cy3_oracle.cpp", "ty_oracle.cpp", "Makefile")]
+    srcs = [os.path.join(_HERE, f) for f in ("cy3_oracle.cpp", "cicy_oracle.cpp", "Makefile")]
     if force or not os.path.exists(_LIB_PATH) or os.path.getmtime(_LIB_PATH) < max(map(os.path.getmtime, srcs)):
         subprocess.check_call(["make", "-s", "-C", _HERE, "liboracle.so"])
     return _LIB_PATH
@@ -101,6 +101,18 @@ def lib():
     L.orc_ty_sigma.restype = d
     L.orc_ty_solve.argtypes = [C.c_int, sz, C.c_int, d, C.c_uint64, _dp, _dp, _dp, C.c_int, vp, vp, sz]
     L.orc_ty_solve.restype = C.c_int
+    L.orc_schoen_sample.argtypes = [C.c_uint64, sz, C.c_int, C.c_int, _dp, _dp, _dp, _ip]
+    L.orc_schoen_sample.restype = sz
+    L.orc_schoen_groebner_lms.argtypes = [_ip, C.c_int]
+    L.orc_schoen_groebner_lms.restype = C.c_int
+    L.orc_schoen_basis.argtypes = [C.c_int, C.c_int, C.c_int, _ip, C.c_int]
+    L.orc_schoen_basis.restype = C.c_int
+    L.orc_schoen_frames.argtypes = [_dp, sz, _dp]
+    L.orc_schoen_sigma.argtypes = [_dp, _dp, _dp, sz, C.c_int, C.c_int, C.c_int, _dp, _dp, vp]
+    L.orc_schoen_sigma.restype = d
+    L.orc_schoen_solve.argtypes = [C.c_int, C.c_int, C.c_int, sz, C.c_int, d, C.c_uint64, _dp, _dp, _dp, C.c_int,
+                                   vp, vp, sz]
+    L.orc_schoen_solve.restype = C.c_int
     _lib = L
     return L
 
@@ -560,7 +572,7 @@ def laplacian_eigs(M: np.ndarray, K: np.ndarray, n_eigs: int = 40, reg: float = 
 
 
 # ---------------------------------------------------------------------------------------------
-# Tian-Yau (oracle/ty_oracle.cpp): the reference's solve_ty_metric path (route34/ty_metric.rs)
+# Tian-Yau (oracle/cicy_oracle.cpp): the reference's solve_ty_metric path (route34/ty_metric.rs)
 # ---------------------------------------------------------------------------------------------
 def ty_rng_u64(seed: int, n: int) -> np.ndarray:
     """First n u64 of ChaCha8Rng::seed_from_u64(seed) (rand_chacha 0.9)."""
@@ -672,6 +684,75 @@ def ty_solve(k: int, n_sample: int, max_iter: int, tol: float, seed: int):
                            hr.ctypes.data, hi.ctypes.data, hr.size)
     if n < 0:
         raise RuntimeError(f"orc_ty_solve failed ({n})")
+    N = int(rec[1])
+    return dict(n_points=int(rec[0]), n_basis=N, iterations_run=int(rec[2]), sigma_fs_identity=rec[3],
+                sigma_final=rec[4], final_donaldson_residual=rec[5], sigma_history=sh[:n].copy(),
+                donaldson_history=rh[:n].copy(), h=(hr + 1j * hi).reshape(N, N))
+
+
+# ---------------------------------------------------------------------------------------------
+# Schoen (oracle/cicy_oracle.cpp): solve_schoen_metric (route34/schoen_metric.rs:766)
+# ---------------------------------------------------------------------------------------------
+def schoen_sample(n: int, seed: int, gpu_stream: bool = False, quotient: bool = True):
+    """SchoenSampler::sample_points (schoen_sampler.rs:482) [+ apply_z3xz3_quotient]; gpu_stream: one Newton
+    attempt per line, the device sampler's layout.  Returns (coords [P,16], omega [P] complex, weight [P],
+    patch [P,3])."""
+    coords = np.empty((n, 16))
+    om = np.empty((n, 2))
+    w = np.empty(n)
+    pa = np.empty((n, 3), dtype=np.int32)
+    P = lib().orc_schoen_sample(int(seed), int(n), int(gpu_stream), int(quotient), coords, om, w, pa)
+    return coords[:P].copy(), (om[:P, 0] + 1j * om[:P, 1]), w[:P].copy(), pa[:P].copy()
+
+
+def schoen_groebner_lms() -> np.ndarray:
+    out = np.zeros(4096 * 8, dtype=np.int32)
+    n = lib().orc_schoen_groebner_lms(out, 4096)
+    return out[: n * 8].reshape(n, 8)
+
+
+def schoen_basis(dx: int, dy: int, dt: int) -> np.ndarray:
+    """build_schoen_invariant_reduced_basis (schoen_metric.rs:1185): [N, 8] exponents."""
+    cap = 20000
+    out = np.zeros(cap * 8, dtype=np.int32)
+    n = lib().orc_schoen_basis(int(dx), int(dy), int(dt), out, cap)
+    return out[: n * 8].reshape(n, 8)
+
+
+def schoen_frames(coords: np.ndarray) -> np.ndarray:
+    """schoen_affine_chart_frame (schoen_metric.rs:2202) per point: [P, 3, 8] complex."""
+    coords = np.ascontiguousarray(coords, dtype=np.float64)
+    P = coords.shape[0]
+    out = np.empty((P, 3, 16))
+    lib().orc_schoen_frames(coords, P, out)
+    return out[..., 0::2] + 1j * out[..., 1::2]
+
+
+def schoen_sigma(coords, omega_sq, w, d, h):
+    """compute_sigma (schoen_metric.rs:1685) for bidegree d = (dx, dy, dt): (sigma, eta [P])."""
+    coords = np.ascontiguousarray(coords, dtype=np.float64)
+    P = coords.shape[0]
+    eta = np.empty(P)
+    s = lib().orc_schoen_sigma(coords, np.ascontiguousarray(omega_sq, dtype=np.float64),
+                               np.ascontiguousarray(w, dtype=np.float64), P, int(d[0]), int(d[1]), int(d[2]),
+                               np.ascontiguousarray(h.real, dtype=np.float64),
+                               np.ascontiguousarray(h.imag, dtype=np.float64), eta.ctypes.data)
+    return s, eta
+
+
+def schoen_solve(d, n_sample: int, max_iter: int, tol: float, seed: int):
+    """solve_schoen_metric (schoen_metric.rs:766) with the spec defaults (cy3_metric_unified.rs:289-320)."""
+    rec = np.zeros(6)
+    cap = max(8, 8 * max_iter + 8)
+    sh = np.zeros(cap)
+    rh = np.zeros(cap)
+    n_est = int(schoen_basis(*d).shape[0])
+    hr = np.zeros(n_est * n_est)
+    hi = np.zeros(n_est * n_est)
+    n = lib().orc_schoen_solve(int(d[0]), int(d[1]), int(d[2]), int(n_sample), int(max_iter), float(tol), int(seed),
+                               rec, sh, rh, cap, hr.ctypes.data, hi.ctypes.data, hr.size)
+    if n < 0:
+        raise RuntimeError(f"orc_schoen_solve failed ({n})")
     N = int(rec[1])
     return dict(n_points=int(rec[0]), n_basis=N, iterations_run=int(rec[2]), sigma_fs_identity=rec[3],
                 sigma_final=rec[4], final_donaldson_residual=rec[5], sigma_history=sh[:n].copy(),

@@ -1,4 +1,4 @@
-// ty_oracle.cpp -- FP64 CPU restatement of the reference's Tian-Yau metric solve.
+// cicy_oracle.cpp -- FP64 CPU restatement of the reference's Tian-Yau and Schoen metric solves.
 //
 // TEST INFRASTRUCTURE ONLY (parity checker and timed CPU baseline), linked into
 // oracle/liboracle.so beside cy3_oracle.cpp and never into the product library.
@@ -6,7 +6,7 @@
 // Reference files (crate substrate_sm_derivation/cy3_solver), cited below as
 //   CS = src/cicy_sampler.rs, TY = src/route34/ty_metric.rs, GB = src/route34/groebner.rs,
 //   HP = src/route34/donaldson_h_pair_sum.rs, SM = src/route34/schoen_metric.rs,
-//   QT = src/quotient.rs.
+//   QT = src/quotient.rs, SS = src/route34/schoen_sampler.rs, ZP = src/route34/z3xz3_projector.rs.
 //
 // Third-party dependencies of the path that are absent from the reference tree, with the
 // versions pinned by its Cargo.lock, restated here from their published algorithms:
@@ -703,17 +703,9 @@ GPoly remainder(GPoly p, const std::vector<GPoly>& basis) {
   return make_poly(rem);
 }
 
-std::vector<Mono> groebner_lms() {
+std::vector<Mono> groebner_lms(const std::vector<std::vector<std::pair<double, Mono>>>& gens) {
   std::vector<GPoly> g;
-  for (int i = 0; i < NH; ++i) {
-    std::vector<std::pair<double, Mono>> terms;
-    for (const Term& t : triple().f[i]) {
-      Mono m;
-      for (int k = 0; k < NC; ++k) m[k] = t.e[k];
-      terms.push_back({1.0, m});
-    }
-    g.push_back(make_poly(terms));
-  }
+  for (const auto& terms : gens) g.push_back(make_poly(terms));
   std::vector<std::pair<int, int>> pairs;
   for (int i = 0; i < (int)g.size(); ++i)
     for (int j = i + 1; j < (int)g.size(); ++j) pairs.push_back({i, j});
@@ -754,8 +746,21 @@ std::vector<Mono> groebner_lms() {
   std::sort(lms.begin(), lms.end(), [](const Mono& a, const Mono& b) { return deglex_cmp(a, b) > 0; });
   return lms;
 }
+// ty_generators (GB:665-703): the Tian-Yau triple with unit coefficients
 const std::vector<Mono>& ty_lms() {
-  static std::vector<Mono> lms = groebner_lms();
+  static std::vector<Mono> lms = [] {
+    std::vector<std::vector<std::pair<double, Mono>>> gens;
+    for (int i = 0; i < NH; ++i) {
+      std::vector<std::pair<double, Mono>> terms;
+      for (const Term& t : triple().f[i]) {
+        Mono m;
+        for (int k = 0; k < NC; ++k) m[k] = t.e[k];
+        terms.push_back({1.0, m});
+      }
+      gens.push_back(terms);
+    }
+    return groebner_lms(gens);
+  }();
   return lms;
 }
 
@@ -871,9 +876,20 @@ bool chart_frame(const TyPt& pt, Cx frame[NF][NC]) {
   return true;
 }
 
+double eta_from_frame(bool frame_ok, const Cx fr[NF][NC], const double* s, const double* d, const double* hr,
+                      const double* hi, int N, double omega_sq);
+
 // compute_eta_at_point (TY:1788-1866)
 double eta_at(const TyPt& pt, const double* s, const double* d, const double* hr, const double* hi, int N,
               double omega_sq) {
+  Cx fr[NF][NC];
+  const bool ok = chart_frame(pt, fr);
+  return eta_from_frame(ok, fr, s, d, hr, hi, N, omega_sq);
+}
+
+// the per-point part of compute_eta_at_point (TY:1788-1866, SM:2092-2160) given the chart frame
+double eta_from_frame(bool frame_ok, const Cx fr[NF][NC], const double* s, const double* d, const double* hr,
+                      const double* hi, int N, double omega_sq) {
   if (!std::isfinite(omega_sq) || omega_sq <= 0.0) return NAN;
   const size_t tn = 2 * (size_t)N;
   double kv, dum;
@@ -894,8 +910,7 @@ double eta_at(const TyPt& pt, const double* s, const double* d, const double* hr
       Cx t2 = divr(dk[i] * conj(dk[j]), ks * ks);
       ga[i][j] = t1 - t2;
     }
-  Cx fr[NF][NC];
-  if (!chart_frame(pt, fr)) return NAN;
+  if (!frame_ok) return NAN;
   Cx gt[NF][NF];
   for (int a = 0; a < NF; ++a)
     for (int b = 0; b < NF; ++b) {
@@ -1230,6 +1245,552 @@ TyData import_points(const double* coords, const double* omega_sq, const double*
   return td;
 }
 
+
+// ---------------------------------------------------------------------------------------
+// Schoen (SS, SM, ZP): the Z/3 x Z/3 quotient of the complete intersection in CP^2 x CP^2 x CP^1,
+// coordinates x_0..x_2, y_0..y_2, t_0, t_1 (SS:99-133), sampler polynomials (SS:188-216)
+//   F1 = (x0^3 + x1^3 + x2^3) t0 + x0 x1 x2 t1,  F2 = (y0^3 + y1^3 + y2^3) t1 + y0 y1 y2 t0
+// ---------------------------------------------------------------------------------------
+constexpr int SNH = 2;
+const int S_LO[3] = {0, 3, 6}, S_HI[3] = {3, 6, 8};
+
+struct SchoenPolys {
+  std::vector<Term> f[SNH];
+  SchoenPolys() {
+    for (int q = 0; q < 2; ++q) {
+      const int b = q == 0 ? 0 : 3, tc = q == 0 ? 6 : 7, to = q == 0 ? 7 : 6;
+      for (int k = 0; k < 3; ++k) {
+        Term t{cx(1.0), {0}};
+        std::memset(t.e, 0, sizeof t.e);
+        t.e[b + k] = 3;
+        t.e[tc] = 1;
+        f[q].push_back(t);
+      }
+      Term t{cx(1.0), {0}};
+      std::memset(t.e, 0, sizeof t.e);
+      t.e[b] = t.e[b + 1] = t.e[b + 2] = 1;
+      t.e[to] = 1;
+      f[q].push_back(t);
+    }
+  }
+};
+const SchoenPolys& spolys() {
+  static SchoenPolys p;
+  return p;
+}
+void s_eval(const Cx x[NC], Cx f[SNH]) {
+  for (int i = 0; i < SNH; ++i) f[i] = eval_poly(spolys().f[i], x);
+}
+void s_jacobian(const Cx x[NC], Cx j[SNH * NC]) {
+  for (int k = 0; k < NC; ++k)
+    for (int i = 0; i < SNH; ++i) j[i * NC + k] = poly_partial(spolys().f[i], x, k);
+}
+double s_residual(const Cx f[SNH]) {
+  double s = 0.0;
+  for (int i = 0; i < SNH; ++i) s += norm_sqr(f[i]);
+  return std::sqrt(s);
+}
+void s_line(const Cx p[NC], const Cx d[SNH][NC], const Cx t[SNH], Cx x[NC]) {
+  for (int k = 0; k < NC; ++k) x[k] = p[k];
+  for (int j = 0; j < SNH; ++j)
+    for (int k = 0; k < NC; ++k) x[k] += t[j] * d[j][k];
+}
+
+// newton_solve_line (SS:642-700): as the Tian-Yau one without the determinant pre-check
+bool s_newton(const Cx p[NC], const Cx d[SNH][NC], Cx t[SNH], Cx x[NC], double* res_out) {
+  const double tol = 1.0e-8;
+  s_line(p, d, t, x);
+  Cx f[SNH];
+  s_eval(x, f);
+  double res = s_residual(f);
+  for (int it = 0; it < 64; ++it) {
+    if (res < tol) {
+      *res_out = res;
+      return true;
+    }
+    Cx jx[SNH * NC], m[SNH * SNH], mi[SNH * SNH];
+    s_jacobian(x, jx);
+    for (int i = 0; i < SNH; ++i)
+      for (int j = 0; j < SNH; ++j) {
+        Cx sm = cx(0.0);
+        for (int k = 0; k < NC; ++k) sm += jx[i * NC + k] * d[j][k];
+        m[i * SNH + j] = sm;
+      }
+    if (!inv_gj(m, SNH, mi)) {
+      *res_out = res;
+      return false;
+    }
+    Cx dt[SNH];
+    for (int r = 0; r < SNH; ++r) {
+      Cx sm = cx(0.0);
+      for (int c = 0; c < SNH; ++c) sm += mi[r * SNH + c] * f[c];
+      dt[r] = -sm;
+    }
+    double step = 1.0;
+    bool accepted = false;
+    for (int q = 0; q < 32; ++q) {
+      Cx tt[SNH], xt[NC], ft[SNH];
+      for (int r = 0; r < SNH; ++r) tt[r] = t[r] + cx(step) * dt[r];
+      s_line(p, d, tt, xt);
+      s_eval(xt, ft);
+      const double rt = s_residual(ft);
+      if (rt < (1.0 - 1.0e-4 * step) * res) {
+        for (int r = 0; r < SNH; ++r) t[r] = tt[r];
+        for (int k = 0; k < NC; ++k) x[k] = xt[k];
+        for (int i = 0; i < SNH; ++i) f[i] = ft[i];
+        res = rt;
+        accepted = true;
+        break;
+      }
+      step *= 0.5;
+    }
+    if (!accepted) {
+      *res_out = res;
+      return false;
+    }
+  }
+  *res_out = res;
+  return res < tol;
+}
+
+struct SPt {
+  Cx x[NC];
+  Cx omega;
+  double weight;
+  int patch[3];  // absolute coordinate index of each factor's largest coordinate
+};
+
+int argmax_range(const Cx* v, int lo, int hi) {
+  int best = lo;
+  double ba = -1.0;
+  for (int k = lo; k < hi; ++k) {
+    const double a = norm(v[k]);
+    if (a > ba) {
+      ba = a;
+      best = k;
+    }
+  }
+  return ba > 0.0 ? best : -1;
+}
+
+// pick_elimination_columns (SS:868-900)
+bool s_pick_elim(const Cx jac[SNH * NC], const int patch[3], int el[SNH]) {
+  bool taken[NC] = {false};
+  for (int f = 0; f < 3; ++f) taken[patch[f]] = true;
+  for (int i = 0; i < SNH; ++i) {
+    int bk = -1;
+    double ba = -1.0;
+    for (int k = 0; k < NC; ++k) {
+      if (taken[k]) continue;
+      const double a = norm(jac[i * NC + k]);
+      if (a > ba) {
+        ba = a;
+        bk = k;
+      }
+    }
+    if (bk < 0 || ba <= 0.0) return false;
+    el[i] = bk;
+    taken[bk] = true;
+  }
+  return true;
+}
+
+// post_process_solved_point (SS:716-850)
+bool s_post_process(const Cx xin[NC], SPt* out) {
+  int patch[3];
+  for (int f = 0; f < 3; ++f) {
+    patch[f] = argmax_range(xin, S_LO[f], S_HI[f]);
+    if (patch[f] < 0) return false;
+  }
+  const double EPS = 2.220446049250313e-16;
+  for (int f = 0; f < 3; ++f)
+    if (norm(xin[patch[f]]) < EPS) return false;
+  Cx xr[NC];
+  for (int f = 0; f < 3; ++f) {
+    const Cx sc = xin[patch[f]];
+    for (int k = S_LO[f]; k < S_HI[f]; ++k) xr[k] = xin[k] / sc;
+  }
+  int near_one = 0;
+  for (int k = 0; k < NC; ++k)
+    if (norm(xr[k] - cx(1.0)) < 1.0e-8) ++near_one;
+  if (near_one > 3) return false;
+  Cx jac[SNH * NC];
+  s_jacobian(xr, jac);
+  int el[SNH];
+  if (!s_pick_elim(jac, patch, el)) return false;
+  Cx om[SNH * SNH];
+  for (int i = 0; i < SNH; ++i)
+    for (int k = 0; k < SNH; ++k) om[i * SNH + k] = jac[i * NC + el[k]];
+  const Cx det_om = det_lu(om, SNH);
+  if (norm(det_om) < EPS) return false;
+  const Cx omega = cx(1.0) / det_om;
+  bool elimd[NC] = {false};
+  for (int f = 0; f < 3; ++f) elimd[patch[f]] = true;
+  for (int k = 0; k < SNH; ++k) elimd[el[k]] = true;
+  int fr[NC], nf = 0;
+  for (int k = 0; k < NC; ++k)
+    if (!elimd[k]) {
+      if (nf >= NF) return false;
+      fr[nf++] = k;
+    }
+  if (nf != NF) return false;
+  Cx jpb[NF * NC];
+  for (int i = 0; i < NF * NC; ++i) jpb[i] = cx(0.0);
+  for (int a = 0; a < NF; ++a) jpb[a * NC + fr[a]] = cx(1.0);
+  Cx oi[SNH * SNH];
+  if (!inv_gj(om, SNH, oi)) return false;
+  for (int a = 0; a < NF; ++a) {
+    Cx b[SNH];
+    for (int i = 0; i < SNH; ++i) b[i] = jac[i * NC + fr[a]];
+    for (int r = 0; r < SNH; ++r) {
+      Cx e = cx(0.0);
+      for (int c = 0; c < SNH; ++c) e += oi[r * SNH + c] * b[c];
+      jpb[a * NC + el[r]] = -e;
+    }
+  }
+  // fs_metric_three_blocks (SS:1090-1135)
+  Cx g[NC * NC];
+  for (int i = 0; i < NC * NC; ++i) g[i] = cx(0.0);
+  for (int f = 0; f < 3; ++f) {
+    double nz = 0.0;
+    for (int k = S_LO[f]; k < S_HI[f]; ++k)
+      if (k != patch[f]) nz += norm_sqr(xr[k]);
+    const double den = (1.0 + nz) * (1.0 + nz);
+    for (int a = S_LO[f]; a < S_HI[f]; ++a) {
+      if (a == patch[f]) continue;
+      for (int b = S_LO[f]; b < S_HI[f]; ++b) {
+        if (b == patch[f]) continue;
+        const double kron = a == b ? 1.0 : 0.0;
+        const Cx num = cx(1.0 + nz) * cx(kron) - xr[a] * conj(xr[b]);
+        g[a * NC + b] = num / cx(den);
+      }
+    }
+  }
+  Cx tmp[NF * NC], gpb[NF * NF];
+  for (int a = 0; a < NF; ++a)
+    for (int b = 0; b < NC; ++b) {
+      Cx sm = cx(0.0);
+      for (int k = 0; k < NC; ++k) sm += jpb[a * NC + k] * g[k * NC + b];
+      tmp[a * NC + b] = sm;
+    }
+  for (int a = 0; a < NF; ++a)
+    for (int b = 0; b < NF; ++b) {
+      Cx sm = cx(0.0);
+      for (int k = 0; k < NC; ++k) sm += tmp[a * NC + k] * conj(jpb[b * NC + k]);
+      gpb[a * NF + b] = sm;
+    }
+  const double det_g = det_lu(gpb, NF).re;
+  if (!std::isfinite(det_g) || std::fabs(det_g) < 1.0e-300) return false;
+  const double weight = norm_sqr(omega) / det_g;
+  if (!std::isfinite(weight) || weight <= 0.0) return false;
+  for (int k = 0; k < NC; ++k) out->x[k] = xr[k];
+  out->omega = omega;
+  out->weight = weight;
+  return true;
+}
+
+// sample_one (SS:429-480)
+bool s_sample_one(Rng& rng, SPt* out) {
+  Cx p[NC], d[SNH][NC];
+  unit_sphere(rng, p);
+  for (int j = 0; j < SNH; ++j) unit_sphere(rng, d[j]);
+  bool have = false;
+  Cx best[NC];
+  double best_res = INFINITY;
+  for (int att = 0; att < 4; ++att) {
+    Cx t[SNH];
+    for (int j = 0; j < SNH; ++j) {
+      const double re = normal(rng);
+      const double im = normal(rng);
+      t[j] = cx(re, im);
+    }
+    Cx x[NC];
+    double res;
+    const bool conv = s_newton(p, d, t, x, &res);
+    if (conv && res < best_res) {
+      best_res = res;
+      for (int k = 0; k < NC; ++k) best[k] = x[k];
+      have = true;
+      if (res < 1.0e-8) break;
+    }
+  }
+  if (!have || best_res >= 1.0e-8) return false;
+  return s_post_process(best, out);
+}
+
+// SchoenMetricPoint's patch indices (SM:1132-1150): argmax over each factor of the rescaled point
+void s_patch_indices(SPt& pt) {
+  for (int f = 0; f < 3; ++f) {
+    int best = S_LO[f];
+    double ba = -1.0;
+    for (int k = S_LO[f]; k < S_HI[f]; ++k) {
+      const double a = norm(pt.x[k]);
+      if (a > ba) {
+        ba = a;
+        best = k;
+      }
+    }
+    pt.patch[f] = best;
+  }
+}
+
+// sample_points (SS:482-503) with normalise_weights (SS:1177-1185, w *= 1/sum) and apply_z3xz3_quotient
+// (SS:555-560); `gpu_stream` draws one Newton attempt per line (52 draws: origin, two directions, t) and keeps
+// the first n accepted lines, the layout of the device sampler
+std::vector<SPt> s_sample(uint64_t seed, size_t n, bool gpu_stream, bool quotient) {
+  Rng rng(seed);
+  std::vector<SPt> out;
+  if (!gpu_stream) {
+    size_t max_total = std::max(n * 64, (size_t)1024), att = 0;
+    while (out.size() < n && att < max_total) {
+      ++att;
+      SPt pt;
+      if (s_sample_one(rng, &pt)) out.push_back(pt);
+    }
+  } else {
+    const size_t lines = std::max(n * 4, (size_t)64);
+    for (size_t l = 0; l < lines && out.size() < n; ++l) {
+      Cx p[NC], d[SNH][NC], t[SNH];
+      unit_sphere(rng, p);
+      for (int j = 0; j < SNH; ++j) unit_sphere(rng, d[j]);
+      for (int j = 0; j < SNH; ++j) {
+        const double re = normal(rng);
+        const double im = normal(rng);
+        t[j] = cx(re, im);
+      }
+      Cx x[NC];
+      double res;
+      if (!s_newton(p, d, t, x, &res)) continue;
+      SPt pt;
+      if (s_post_process(x, &pt)) out.push_back(pt);
+    }
+  }
+  double sum = 0.0;
+  for (auto& q : out) sum += q.weight;
+  if (std::isfinite(sum) && sum > 0.0) {
+    const double inv = 1.0 / sum;
+    for (auto& q : out) q.weight *= inv;
+  }
+  if (quotient) {
+    const double inv_k = 1.0 / 9.0;
+    for (auto& q : out) q.weight *= inv_k;
+  }
+  for (auto& q : out) s_patch_indices(q);
+  return out;
+}
+
+// schoen_generators (GB:705-738): the ideal the basis is reduced by (sign pattern + - - on the t_1 terms)
+const std::vector<Mono>& schoen_lms() {
+  static std::vector<Mono> lms = [] {
+    std::vector<std::vector<std::pair<double, Mono>>> gens(2);
+    for (int q = 0; q < 2; ++q)
+      for (int k = 0; k < 3; ++k) {
+        Mono e{};
+        e[3 * q + k] = 3;
+        e[6] = 1;
+        gens[q].push_back({1.0, e});
+        Mono e2{};
+        e2[3 * q + k] = 3;
+        e2[7] = 1;
+        gens[q].push_back({k == 0 ? 1.0 : -1.0, e2});
+      }
+    return groebner_lms(gens);
+  }();
+  return lms;
+}
+
+// build_schoen_invariant_reduced_basis (SM:1185-1210) over enumerate_bidegree_monomials (ZP:298-315),
+// Gamma-invariance = alpha (m1 + 2 m2 + m4 + 2 m5) mod 3 == 0 and beta m7 mod 3 == 0 (ZP:100-186)
+std::vector<Mono> s_basis(int dx, int dy, int dt) {
+  std::vector<Mono> out;
+  const auto& lms = schoen_lms();
+  for (int a0 = 0; a0 <= dx; ++a0)
+    for (int a1 = 0; a1 <= dx - a0; ++a1)
+      for (int b0 = 0; b0 <= dy; ++b0)
+        for (int b1 = 0; b1 <= dy - b0; ++b1)
+          for (int c0 = 0; c0 <= dt; ++c0) {
+            Mono m = {a0, a1, dx - a0 - a1, b0, b1, dy - b0 - b1, c0, dt - c0};
+            if ((m[1] + 2 * m[2] + m[4] + 2 * m[5]) % 3 != 0 || m[7] % 3 != 0) continue;
+            bool in_ideal = false;
+            for (auto& l : lms)
+              if (divides(l, m)) {
+                in_ideal = true;
+                break;
+              }
+            if (!in_ideal) out.push_back(m);
+          }
+  return out;
+}
+
+// schoen_affine_chart_frame (SM:2202-2270)
+bool s_chart_frame(const SPt& pt, Cx frame[NF][NC]) {
+  Cx jac[SNH * NC];
+  s_jacobian(pt.x, jac);
+  int el[SNH];
+  if (!s_pick_elim(jac, pt.patch, el)) return false;
+  bool taken[NC] = {false};
+  for (int f = 0; f < 3; ++f) taken[pt.patch[f]] = true;
+  for (int i = 0; i < SNH; ++i) taken[el[i]] = true;
+  int fr[NF], nf = 0;
+  for (int k = 0; k < NC; ++k)
+    if (!taken[k]) {
+      if (nf >= NF) return false;
+      fr[nf++] = k;
+    }
+  if (nf != NF) return false;
+  Cx je[SNH * SNH], ji[SNH * SNH];
+  for (int i = 0; i < SNH; ++i)
+    for (int c = 0; c < SNH; ++c) je[i * SNH + c] = jac[i * NC + el[c]];
+  if (!inv_gj(je, SNH, ji)) return false;
+  for (int a = 0; a < NF; ++a)
+    for (int k = 0; k < NC; ++k) frame[a][k] = cx(0.0);
+  for (int a = 0; a < NF; ++a) {
+    frame[a][fr[a]] = cx(1.0);
+    Cx b[SNH];
+    for (int i = 0; i < SNH; ++i) b[i] = jac[i * NC + fr[a]];
+    for (int c = 0; c < SNH; ++c) {
+      Cx e = cx(0.0);
+      for (int i = 0; i < SNH; ++i) e += ji[c * SNH + i] * b[i];
+      frame[a][el[c]] = -e;
+    }
+  }
+  return true;
+}
+
+struct SData {
+  std::vector<SPt> pts;
+  std::vector<double> w, om2;
+  std::vector<Mono> basis;
+  std::vector<double> S, D;
+};
+
+void s_build(SData& sd) {
+  const size_t P = sd.pts.size();
+  const int N = (int)sd.basis.size();
+  int kmax = 0;
+  for (auto& m : sd.basis)
+    for (int k = 0; k < NC; ++k) kmax = std::max(kmax, m[k]);
+  sd.S.assign(P * 2 * N, 0.0);
+  sd.D.assign(P * NC * 2 * N, 0.0);
+  par_for(P, [&](size_t p) { sections_at(sd.pts[p].x, sd.basis, kmax, sd.S.data() + p * 2 * N, sd.D.data() + p * NC * 2 * N); });
+}
+
+double s_sigma(const SData& sd, const double* hr, const double* hi, double* eta_out) {
+  const size_t P = sd.pts.size();
+  const int N = (int)sd.basis.size();
+  std::vector<double> eta(P);
+  par_for(P, [&](size_t p) {
+    Cx fr[NF][NC];
+    const bool ok = s_chart_frame(sd.pts[p], fr);
+    eta[p] = eta_from_frame(ok, fr, sd.S.data() + p * 2 * N, sd.D.data() + p * NC * 2 * N, hr, hi, N, sd.om2[p]);
+  });
+  if (eta_out) std::copy(eta.begin(), eta.end(), eta_out);
+  return sigma_reduce(eta.data(), sd.w.data(), P);
+}
+
+SData s_import(const double* coords, const double* omega_sq, const double* weight, size_t P, int dx, int dy, int dt) {
+  SData sd;
+  sd.pts.resize(P);
+  sd.w.assign(weight, weight + P);
+  sd.om2.assign(omega_sq, omega_sq + P);
+  for (size_t p = 0; p < P; ++p) {
+    for (int q = 0; q < NC; ++q) sd.pts[p].x[q] = cx(coords[p * 16 + 2 * q], coords[p * 16 + 2 * q + 1]);
+    s_patch_indices(sd.pts[p]);
+    sd.pts[p].weight = weight[p];
+  }
+  sd.basis = s_basis(dx, dy, dt);
+  return sd;
+}
+// The balancing loop of solve_ty_metric / solve_schoen_metric (TY:555-720, SM:830-1000) on a section table:
+// damping (static, or the adaptive ramp of SM:571-625), the min-residual snapshot and catastrophe guard,
+// sigma after every iteration through `sig`.  Fills rec / histories / h as orc_ty_solve documents.
+template <class SigmaFn>
+int solve_loop(const double* S, const double* w, size_t P, int N, SigmaFn sig, bool adaptive, int max_iter, double tol,
+               double* rec, double* sig_hist, double* res_hist, int hist_cap, double* h_re, double* h_im,
+               size_t h_cap) {
+  const size_t NN = (size_t)N * N;
+  std::vector<double> hr(NN, 0.0), hi(NN, 0.0);
+  for (int a = 0; a < N; ++a) hr[a * N + a] = 1.0;
+  double alpha = adaptive ? 0.3 : 1.0, a_min = 0.05, a_max = 1.0, last_res = INFINITY;
+  int streak = 0;
+  int eff_iter = adaptive ? max_iter * std::max(7, 2) : max_iter;
+  double sig_fs = sig(hr.data(), hi.data());
+  double min_res = INFINITY, final_res = INFINITY;
+  std::vector<double> mhr = hr, mhi = hi;
+  int min_it = 0, bad = 0, iters = 0;
+  std::vector<double> sh, rh;
+  for (int it = 0; it < eff_iter; ++it) {
+    double res = donaldson_iteration(S, w, P, N, hr.data(), hi.data(), alpha);
+    if (adaptive) {
+      if (std::isfinite(res)) {
+        if (std::isfinite(last_res)) {
+          if (res < 0.95 * last_res) {
+            if (++streak >= 3) {
+              alpha = std::min(alpha * 1.5, a_max);
+              streak = 0;
+            }
+          } else if (res > 1.05 * last_res) {
+            alpha = std::max(alpha * 0.7, a_min);
+            streak = 0;
+          }
+        }
+      }
+      last_res = res;
+    }
+    if (!std::isfinite(res)) {
+      if (std::isfinite(min_res)) {
+        hr = mhr;
+        hi = mhi;
+        rh.push_back(min_res);
+        sh.push_back(sig(hr.data(), hi.data()));
+        final_res = min_res;
+        iters = min_it;
+        break;
+      }
+      return -3;
+    }
+    rh.push_back(res);
+    sh.push_back(sig(hr.data(), hi.data()));
+    final_res = res;
+    iters = it + 1;
+    if (res < min_res) {
+      min_res = res;
+      mhr = hr;
+      mhi = hi;
+      min_it = iters;
+      bad = 0;
+    } else if (std::isfinite(min_res) && min_res < 1.0e-2 && res > 100.0 * min_res) {
+      if (++bad >= 5) {
+        hr = mhr;
+        hi = mhi;
+        rh.push_back(min_res);
+        sh.push_back(sig(hr.data(), hi.data()));
+        final_res = min_res;
+        iters = min_it;
+        break;
+      }
+    } else {
+      bad = 0;
+    }
+    if (res < tol) break;
+  }
+  rec[0] = (double)P;
+  rec[1] = (double)N;
+  rec[2] = (double)iters;
+  rec[3] = sig_fs;
+  rec[4] = sh.empty() ? NAN : sh.back();
+  rec[5] = final_res;
+  for (int i = 0; i < (int)sh.size() && i < hist_cap; ++i) {
+    sig_hist[i] = sh[i];
+    res_hist[i] = rh[i];
+  }
+  if (h_re && NN <= h_cap) {
+    std::copy(hr.begin(), hr.end(), h_re);
+    std::copy(hi.begin(), hi.end(), h_im);
+  }
+  return (int)sh.size();
+}
+
 }  // namespace
 
 extern "C" {
@@ -1364,88 +1925,86 @@ int orc_ty_solve(int k, size_t n_sample, int max_iter, double tol, uint64_t seed
   const int N = (int)td.basis.size();
   if (N == 0) return -2;
   build_sections(td, true);
-  const size_t NN = (size_t)N * N, P = td.pts.size();
-  std::vector<double> hr(NN, 0.0), hi(NN, 0.0);
-  for (int a = 0; a < N; ++a) hr[a * N + a] = 1.0;
-  bool adaptive = k >= 4;
-  double alpha = adaptive ? 0.3 : 1.0, a_min = 0.05, a_max = 1.0, last_res = INFINITY;
-  int streak = 0;
-  int eff_iter = adaptive ? max_iter * std::max(7, 2) : max_iter;
-  double sig_fs = sigma_of(td, hr.data(), hi.data(), nullptr);
-  double min_res = INFINITY, final_res = INFINITY;
-  std::vector<double> mhr = hr, mhi = hi;
-  int min_it = 0, bad = 0, iters = 0;
-  std::vector<double> sh, rh;
-  for (int it = 0; it < eff_iter; ++it) {
-    double res = donaldson_iteration(td.S.data(), td.w.data(), P, N, hr.data(), hi.data(), alpha);
-    if (adaptive) {
-      if (std::isfinite(res)) {
-        if (std::isfinite(last_res)) {
-          if (res < 0.95 * last_res) {
-            if (++streak >= 3) {
-              alpha = std::min(alpha * 1.5, a_max);
-              streak = 0;
-            }
-          } else if (res > 1.05 * last_res) {
-            alpha = std::max(alpha * 0.7, a_min);
-            streak = 0;
-          }
-        }
-      }
-      last_res = res;
+  return solve_loop(td.S.data(), td.w.data(), td.pts.size(), N,
+                    [&](const double* hr, const double* hi) { return sigma_of(td, hr, hi, nullptr); }, k >= 4,
+                    max_iter, tol, rec, sig_hist, res_hist, hist_cap, h_re, h_im, h_cap);
+}
+
+// Schoen entry points: coords [n][16] (x_0..x_2, y_0..y_2, t_0, t_1 rescaled), omega [n] complex, weight [n],
+// patch [n][3] absolute indices.  Returns the count.
+size_t orc_schoen_sample(uint64_t seed, size_t n, int gpu_stream, int quotient, double* coords, double* omega,
+                         double* weight, int* patch) {
+  std::vector<SPt> pts = s_sample(seed, n, gpu_stream != 0, quotient != 0);
+  for (size_t p = 0; p < pts.size(); ++p) {
+    for (int k = 0; k < NC; ++k) {
+      coords[p * 16 + 2 * k] = pts[p].x[k].re;
+      coords[p * 16 + 2 * k + 1] = pts[p].x[k].im;
     }
-    if (!std::isfinite(res)) {
-      if (std::isfinite(min_res)) {
-        hr = mhr;
-        hi = mhi;
-        rh.push_back(min_res);
-        sh.push_back(sigma_of(td, hr.data(), hi.data(), nullptr));
-        final_res = min_res;
-        iters = min_it;
-        break;
-      }
-      return -3;
+    if (omega) {
+      omega[2 * p] = pts[p].omega.re;
+      omega[2 * p + 1] = pts[p].omega.im;
     }
-    rh.push_back(res);
-    sh.push_back(sigma_of(td, hr.data(), hi.data(), nullptr));
-    final_res = res;
-    iters = it + 1;
-    if (res < min_res) {
-      min_res = res;
-      mhr = hr;
-      mhi = hi;
-      min_it = iters;
-      bad = 0;
-    } else if (std::isfinite(min_res) && min_res < 1.0e-2 && res > 100.0 * min_res) {
-      if (++bad >= 5) {
-        hr = mhr;
-        hi = mhi;
-        rh.push_back(min_res);
-        sh.push_back(sigma_of(td, hr.data(), hi.data(), nullptr));
-        final_res = min_res;
-        iters = min_it;
-        break;
+    if (weight) weight[p] = pts[p].weight;
+    if (patch)
+      for (int f = 0; f < 3; ++f) patch[3 * p + f] = pts[p].patch[f];
+  }
+  return pts.size();
+}
+
+int orc_schoen_groebner_lms(int* out, int cap) {
+  const auto& l = schoen_lms();
+  for (int i = 0; i < (int)l.size() && i < cap; ++i)
+    for (int k = 0; k < NC; ++k) out[i * NC + k] = l[i][k];
+  return (int)l.size();
+}
+
+int orc_schoen_basis(int dx, int dy, int dt, int* out, int cap) {
+  std::vector<Mono> b = s_basis(dx, dy, dt);
+  for (int i = 0; i < (int)b.size() && i < cap; ++i)
+    for (int q = 0; q < NC; ++q) out[i * NC + q] = b[i][q];
+  return (int)b.size();
+}
+
+void orc_schoen_frames(const double* coords, size_t P, double* out) {
+  for (size_t p = 0; p < P; ++p) {
+    SPt pt;
+    for (int q = 0; q < NC; ++q) pt.x[q] = cx(coords[p * 16 + 2 * q], coords[p * 16 + 2 * q + 1]);
+    s_patch_indices(pt);
+    Cx fr[NF][NC];
+    const bool ok = s_chart_frame(pt, fr);
+    for (int a = 0; a < NF; ++a)
+      for (int q = 0; q < NC; ++q) {
+        out[p * 48 + a * 16 + 2 * q] = ok ? fr[a][q].re : NAN;
+        out[p * 48 + a * 16 + 2 * q + 1] = ok ? fr[a][q].im : NAN;
       }
-    } else {
-      bad = 0;
-    }
-    if (res < tol) break;
   }
-  rec[0] = (double)P;
-  rec[1] = (double)N;
-  rec[2] = (double)iters;
-  rec[3] = sig_fs;
-  rec[4] = sh.empty() ? NAN : sh.back();
-  rec[5] = final_res;
-  for (int i = 0; i < (int)sh.size() && i < hist_cap; ++i) {
-    sig_hist[i] = sh[i];
-    res_hist[i] = rh[i];
+}
+
+double orc_schoen_sigma(const double* coords, const double* omega_sq, const double* weight, size_t P, int dx, int dy,
+                        int dt, const double* h_re, const double* h_im, double* eta) {
+  SData sd = s_import(coords, omega_sq, weight, P, dx, dy, dt);
+  s_build(sd);
+  return s_sigma(sd, h_re, h_im, eta);
+}
+
+// solve_schoen_metric (SM:766-1000) with the reference's default damping (adaptive when dx + dy + dt >= 10,
+// SM:649-665), no Tikhonov shift, no Adam; outputs as orc_ty_solve.
+int orc_schoen_solve(int dx, int dy, int dt, size_t n_sample, int max_iter, double tol, uint64_t seed, double* rec,
+                     double* sig_hist, double* res_hist, int hist_cap, double* h_re, double* h_im, size_t h_cap) {
+  SData sd;
+  sd.pts = s_sample(seed, n_sample, false, true);
+  if (sd.pts.size() < n_sample / 2) return -1;
+  for (auto& q : sd.pts) {
+    sd.w.push_back(q.weight);
+    sd.om2.push_back(norm_sqr(q.omega));
   }
-  if (h_re && NN <= h_cap) {
-    std::copy(hr.begin(), hr.end(), h_re);
-    std::copy(hi.begin(), hi.end(), h_im);
-  }
-  return (int)sh.size();
+  sd.basis = s_basis(dx, dy, dt);
+  const int N = (int)sd.basis.size();
+  if (N == 0) return -2;
+  s_build(sd);
+  return solve_loop(sd.S.data(), sd.w.data(), sd.pts.size(), N,
+                    [&](const double* hr, const double* hi) { return s_sigma(sd, hr, hi, nullptr); },
+                    dx + dy + dt >= 10, max_iter, tol, rec, sig_hist, res_hist, hist_cap, h_re, h_im, h_cap);
 }
 
 }  // extern "C"

@@ -20,6 +20,9 @@ use next to this script; the fixtures are committed, so the tests never read the
   solve_ty_metric (src/route34/ty_metric.rs:461; spec of src/route34/cy3_metric_unified.rs:242-261): k = 3,
   20 seeds at n = 40,000 and 3 seeds at n = 2,000 (100 and 30 iterations, tolerance 1e-6), and the
   determinism record at n = 200 (5 iterations; bit patterns decoded to floats).
+* the same three files -> schoen_kat.json: the Schoen records of solve_schoen_metric
+  (src/route34/schoen_metric.rs:766; spec of src/route34/cy3_metric_unified.rs:289-320) at (d_x, d_y, d_t) =
+  (3, 3, 1), the tuple the reference uses for k = 3.
 """
 import json
 import struct
@@ -71,7 +74,7 @@ def p5_3(src_dir):
     return "p5_3_kat.json", out
 
 
-def ty(src_dir):
+def ty(src_dir, candidate="TY"):
     out = {
         "source": ["substrate_sm_derivation/cy3_solver/output/p5_10_ty_schoen_5sigma.json",
                    "substrate_sm_derivation/cy3_solver/output/bit_exact_fix/p5_10_xoshiro_reduced.json",
@@ -84,7 +87,7 @@ def ty(src_dir):
     for name, max_iter in (("p5_10_ty_schoen_5sigma.json", None), (os.path.join("bit_exact_fix", "p5_10_xoshiro_reduced.json"), 30)):
         ref = json.load(open(os.path.join(src_dir, name)))
         for cand in ref["candidates"]:
-            if cand["candidate"] != "TY":
+            if cand["candidate"] != candidate:
                 continue
             for rec in cand["per_seed"]:
                 out["records"].append({
@@ -97,7 +100,7 @@ def ty(src_dir):
     gold = json.load(open(os.path.join(src_dir, os.pardir, "tests", "data", "p5_10_determinism_golden.json")))
     f64 = lambda b: struct.unpack("<d", struct.pack("<Q", b))[0]
     for rec in gold["records"]:
-        if rec["candidate"] != "TY":
+        if rec["candidate"] != candidate:
             continue
         out["records"].append({
             "k": rec["k"], "n_pts": rec["n_pts"], "seed": rec["seed"], "max_iter": rec["donaldson_iters"],
@@ -105,11 +108,21 @@ def ty(src_dir):
             "sigma_fs_identity": f64(rec["sigma_fs_identity_bits"]), "sigma_final": f64(rec["sigma_final_bits"]),
             "final_donaldson_residual": f64(rec["final_donaldson_residual_bits"]),
         })
+    if candidate != "TY":
+        out["protocol"] = ("SchoenSolver.solve_metric(Cy3MetricSpec::Schoen { d_x: 3, d_y: 3, d_t: 1, n_sample, max_iter, "
+                           "donaldson_tol, seed }): SchoenSampler::sample_points + Z/3 x Z/3 quotient, invariant "
+                           "Groebner-reduced basis, h = I, donaldson_iteration until residual < tol, sigma after every "
+                           "iteration")
+        return "schoen_kat.json", out
     return "ty_kat.json", out
 
 
+def schoen(src_dir):
+    return ty(src_dir, "Schoen")
+
+
 def main(src_dir):
-    for make in (p5_9, p5_3, ty):
+    for make in (p5_9, p5_3, ty, schoen):
         name, out = make(src_dir)
         dst = os.path.join(HERE, name)
         json.dump(out, open(dst, "w"), indent=1)

@@ -1,4 +1,4 @@
-"""CPU tests of the Tian-Yau restatement in the oracle (oracle/ty_oracle.cpp) against the reference's
+"""CPU tests of the Tian-Yau restatement in the oracle (oracle/cicy_oracle.cpp) against the reference's
 records (tests/golden/ty_kat.json) and the invariants the reference's own tests check
 (src/cicy_sampler.rs:1160-1680, src/route34/ty_metric.rs:2600-3286).
 
