@@ -179,3 +179,23 @@ def test_schoen_device_sampler_matches_oracle_stream(ty, n, seed):
     assert np.abs(og / np.abs(om) ** 2 - 1).max() < 1e-12
     assert np.abs(wg / w - 1).max() < 1e-12
     assert abs(wg.sum() - 1.0 / 9.0) < 1e-14
+
+
+def test_sigma_of_an_indefinite_metric_matches_oracle(ty):
+    """sigma factors h (h = L L^H); a metric that is not positive definite goes through h itself."""
+    c, om, w, zw = oracle.ty_sample(1500, 8)
+    o2 = np.abs(om) ** 2
+    ws = _ws(ty, 3)
+    ws.set_points(c, o2, w)
+    N = ws.n_basis
+    rng = np.random.default_rng(3)
+    a = rng.standard_normal((N, N)) + 1j * rng.standard_normal((N, N))
+    h = np.eye(N) + 0.05 * (a + a.conj().T)
+    h[0, 0] = -0.5  # indefinite
+    ws.h = h
+    so, _ = oracle.ty_sigma(c, o2, w, 3, h)
+    assert _rel(ws.sigma(), so) < 1e-9
+    hp = np.eye(N) + 0.01 * (a + a.conj().T)  # positive definite
+    ws.h = hp
+    so, _ = oracle.ty_sigma(c, o2, w, 3, hp)
+    assert _rel(ws.sigma(), so) < 1e-10
