@@ -116,6 +116,23 @@ cy3q_status cy3q_schoen_config_default(cy3q_schoen_config* cfg);
 cy3q_status cy3q_schoen_basis(int d_x, int d_y, int d_t, int* n, int* exps, int cap);
 cy3q_status cy3q_schoen_create(const cy3q_schoen_config* cfg, cy3q_ty** out);
 
+/*
+ * Metric cache for both geometries (route34/metric_cache.rs, load_or_solve_ty / load_or_solve_schoen :242-310).
+ * The file name is the reference's: ty_k{k}_n{n}_i{max_iter}_seed{seed}_{h} or
+ * schoen_dx{..}_dy{..}_dt{..}_n{n}_i{max_iter}_seed{seed}_{h}, h = the first 16 hex digits of SHA-256 of the
+ * reference's key JSON (TyKeyMaterial / SchoenKeyMaterial, metric_cache.rs:131-226), with the library's own
+ * payload format (extension .cy3m: key JSON, basis size, sigma, residual, the SHA-256 of the sample cloud as
+ * sha256_points computes it, h_re and h_im, a checksum), written under a temporary name and renamed.
+ * Loading checks the key, the basis size, the checksum and, when the handle holds points, the cloud hash
+ * (CY3Q_ERR_MISS otherwise); strict mode refuses sigma >= CY3Q_SIGMA_QUALITY_THRESHOLD (CY3Q_ERR_STALE).
+ */
+cy3q_status cy3q_ty_cache_file(const cy3q_ty_config* cfg, const char* root, char* path, size_t len);
+cy3q_status cy3q_schoen_cache_file(const cy3q_schoen_config* cfg, const char* root, char* path, size_t len);
+/* sha256_points (ty_metric.rs:2569, schoen_metric.rs:2630) of the handle's points, 64 hex digits + NUL. */
+cy3q_status cy3q_ty_cloud_sha256(cy3q_ty* t, char* hex65);
+cy3q_status cy3q_ty_cache_store(cy3q_ty* t, const char* root, double sigma_final, double residual);
+cy3q_status cy3q_ty_cache_load(cy3q_ty* t, const char* root, int strict, double* sigma_final, double* residual);
+
 #ifdef __cplusplus
 }
 #endif

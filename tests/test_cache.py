@@ -62,3 +62,32 @@ def test_every_key_field_changes_the_path(cy):
                dict(reduced_basis=0), dict(precision=0), dict(max_iter=21), dict(tol=1e-12)]
     paths = {cy.cache_path("c", _key(cy, **c)) for c in changes}
     assert base not in paths and len(paths) == len(changes)
+
+
+def test_ty_and_schoen_cache_names_follow_the_reference():
+    """ty_cache_path / schoen_cache_path (route34/metric_cache.rs:174-226): readable fields and the first 16 hex
+    digits of SHA-256 of the serde_json encoding of the key material (field order, no spaces)."""
+    import hashlib
+    import json
+    import struct
+
+    from papers_b200 import ty
+
+    def ref_name(kind, fields, stem):
+        js = json.dumps(fields, separators=(",", ":"))
+        return f"{stem}_{hashlib.sha256(js.encode()).hexdigest()[:16]}.cy3m"
+
+    tolbits = struct.unpack("<Q", struct.pack("<d", 1e-6))[0]
+    c = ty.TyMetricConfig(k_degree=3, n_sample=40000, max_iter=100, donaldson_tol=1e-6, seed=42)
+    want = ref_name("ty", {"schema_version": 1, "manifold": "tian_yau_z3", "k_degree": 3, "n_sample": 40000,
+                           "max_iter": 100, "donaldson_tol_bits": tolbits, "seed": 42, "apply_z3_quotient": True},
+                    "ty_k3_n40000_i100_seed42")
+    assert ty.cache_path("/tmp/cc", c) == "/tmp/cc/" + want
+    s = ty.SchoenMetricConfig(d_x=3, d_y=3, d_t=1, n_sample=2000, max_iter=30, donaldson_tol=1e-6, seed=7)
+    want = ref_name("schoen", {"schema_version": 1, "manifold": "schoen_z3xz3", "d_x": 3, "d_y": 3, "d_t": 1,
+                               "n_sample": 2000, "max_iter": 30, "donaldson_tol_bits": tolbits, "seed": 7,
+                               "apply_z3xz3_quotient": True, "schoen_bundle_canonical": False},
+                    "schoen_dx3_dy3_dt1_n2000_i30_seed7")
+    assert ty.cache_path("", s) == want
+    assert ty.cache_path("/x", ty.TyMetricConfig(k_degree=3, n_sample=40000, max_iter=100, donaldson_tol=1e-6,
+                                                 seed=43)) != "/x/" + want

@@ -199,3 +199,42 @@ def test_sigma_of_an_indefinite_metric_matches_oracle(ty):
     ws.h = hp
     so, _ = oracle.ty_sigma(c, o2, w, 3, hp)
     assert _rel(ws.sigma(), so) < 1e-10
+
+
+def test_metric_cache_round_trip_and_guards(ty, tmp_path):
+    """load_or_solve_ty / load_or_solve_schoen (route34/metric_cache.rs:242-310)."""
+    root = str(tmp_path)
+    cfg = ty.TyMetricConfig(k_degree=3, n_sample=3000, max_iter=30, donaldson_tol=1e-6, seed=4)
+    r1, out1, p1 = ty.load_or_solve(root, cfg)
+    assert out1 == "miss" and p1.endswith(".cy3m")
+    r2, out2, p2 = ty.load_or_solve(root, cfg)
+    assert out2 == "hit" and p2 == p1
+    assert np.array_equal(r2["balanced_h"], r1["balanced_h"]) and r2["sigma_final"] == r1["sigma_final"]
+    # a fresh handle of another seed misses; one whose points differ from the recorded cloud misses too
+    ws = ty.TyWorkspace(ty.TyMetricConfig(k_degree=3, n_sample=3000, max_iter=30, donaldson_tol=1e-6, seed=5))
+    ws.sample()
+    with pytest.raises(ty.Cy3qError) as e:
+        ws.cache_load(root)
+    assert e.value.status == 12
+    ws4 = ty.TyWorkspace(cfg)
+    cc, om, ww, _ = oracle.ty_sample(3000, 11, gpu_stream=True)
+    ws4.set_points(cc, np.abs(om) ** 2, ww)
+    with pytest.raises(ty.Cy3qError) as e:
+        ws4.cache_load(root)
+    assert e.value.status == 12
+    # strict quality: sigma of this solve is far above 1e-3
+    with pytest.raises(ty.Cy3qError) as e:
+        ty.load_or_solve(root, cfg, strict_quality=True)
+    assert e.value.status == 13
+    # the cloud hash is the reference's sha256_points over the big-endian coordinates
+    import hashlib
+
+    ws5 = ty.TyWorkspace(cfg)
+    ws5.sample()
+    pts, _, _ = ws5.points()
+    assert ws5.cloud_sha256() == hashlib.sha256(pts.astype(">f8").tobytes()).hexdigest()
+    # Schoen: the same guards through its own file name
+    scfg = ty.SchoenMetricConfig(n_sample=2000, max_iter=10, donaldson_tol=1e-6, seed=4)
+    s1, so1, sp1 = ty.load_or_solve(root, scfg)
+    s2, so2, sp2 = ty.load_or_solve(root, scfg)
+    assert so1 == "miss" and so2 == "hit" and sp1 != p1 and np.array_equal(s1["balanced_h"], s2["balanced_h"])
