@@ -473,8 +473,10 @@ def cicy_run(a, dev, cfg, warm_cfg, basis, sigma_fn, cpu: bool, record_s: float)
 
 
 def ty_run(a, dev, cpu: bool):
-    """Tian-Yau k = 3 and Schoen (3, 3, 1) at 40,000 points, up to 100 iterations to 1e-6 (the reference's
-    P5.10 production setting; its records: 20.1 s and 3.8 s per seed for seed 42)."""
+    """Tian-Yau k = 3 and k = 4 and Schoen (3, 3, 1) at 40,000 points, up to 100 iterations to 1e-6 (the reference's
+    P5.10 production settings; its records for seed 42: 20.1 s (k = 3, CPU path), 114.5 s (k = 4, its GPU path,
+    adaptive damping) and 3.8 s per seed).  The k = 4 solve has no CPU column (the oracle's sigma at N = 200 and
+    40,000 points takes minutes)."""
     from papers_b200 import ty
 
     out = {}
@@ -487,6 +489,10 @@ def ty_run(a, dev, cpu: bool):
     warm = ty.TyMetricConfig(k_degree=3, n_sample=2000, max_iter=3, donaldson_tol=1e-6, seed=a.seed, device=dev)
     out["tian_yau"] = cicy_run(a, dev, cfg, warm, tyb,
                                lambda c, o2, w, h: __import__("oracle").ty_sigma(c, o2, w, 3, h), cpu, 20.11)
+    cfg4 = ty.TyMetricConfig(k_degree=4, n_sample=a.ty_points, max_iter=100, donaldson_tol=1e-6, seed=a.seed,
+                             device=dev)
+    warm4 = ty.TyMetricConfig(k_degree=4, n_sample=2000, max_iter=1, donaldson_tol=1e-6, seed=a.seed, device=dev)
+    out["tian_yau_k4"] = cicy_run(a, dev, cfg4, warm4, None, None, False, 114.49)
     scfg = ty.SchoenMetricConfig(n_sample=a.ty_points, max_iter=100, donaldson_tol=1e-6, seed=a.seed, device=dev)
     swarm = ty.SchoenMetricConfig(n_sample=2000, max_iter=3, donaldson_tol=1e-6, seed=a.seed, device=dev)
     out["schoen"] = cicy_run(a, dev, scfg, swarm, scb,
@@ -812,6 +818,9 @@ def main():
                 "schoen": pick((tian_yau or {}).get("schoen"), ["solve_s", "iterations", "sigma_final",
                                                                "gpu_ms_per_iteration", "cpu_s_per_iteration"])
                 if tian_yau and "schoen" in tian_yau else None,
+                "tian_yau_k4": pick((tian_yau or {}).get("tian_yau_k4"), ["solve_s", "iterations", "sigma_final",
+                                                                         "reference_record_s"])
+                if tian_yau and "tian_yau_k4" in tian_yau else None,
                 "residual_last": residuals[-1], "sigma": sig,
                 "sigma_evals_per_s": sigma_per_s, "sigma_evals_per_s_fp64": sigma64_per_s,
                 "fp64_iters_per_s": fp64_per_s, "speedup_vs_fp64": (value / fp64_per_s) if fp64_per_s else None,

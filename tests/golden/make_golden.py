@@ -18,8 +18,9 @@ use next to this script; the fixtures are committed, so the tests never read the
 * p5_10_ty_schoen_5sigma.json, bit_exact_fix/p5_10_xoshiro_reduced.json and
   ../tests/data/p5_10_determinism_golden.json -> ty_kat.json: the Tian-Yau records of the reference's
   solve_ty_metric (src/route34/ty_metric.rs:461; spec of src/route34/cy3_metric_unified.rs:242-261): k = 3,
-  20 seeds at n = 40,000 and 3 seeds at n = 2,000 (100 and 30 iterations, tolerance 1e-6), and the
-  determinism record at n = 200 (5 iterations; bit patterns decoded to floats).
+  20 seeds at n = 40,000 and 3 seeds at n = 2,000 (100 and 30 iterations, tolerance 1e-6), the 20-seed runs
+  at k = 4 and k = 5 (p5_10_k4_adaptive.json, p5_10_k5_damped.json: 40,000 points, 100 / 200 iterations), and
+  the determinism record at n = 200 (5 iterations; bit patterns decoded to floats).
 * the same three files -> schoen_kat.json: the Schoen records of solve_schoen_metric
   (src/route34/schoen_metric.rs:766; spec of src/route34/cy3_metric_unified.rs:289-320) at (d_x, d_y, d_t) =
   (3, 3, 1), the tuple the reference uses for k = 3.
@@ -84,7 +85,8 @@ def ty(src_dir, candidate="TY"):
                     "donaldson_iteration until residual < tol, sigma after every iteration",
         "records": [],
     }
-    for name, max_iter in (("p5_10_ty_schoen_5sigma.json", None), (os.path.join("bit_exact_fix", "p5_10_xoshiro_reduced.json"), 30)):
+    for name, max_iter in (("p5_10_ty_schoen_5sigma.json", None), (os.path.join("bit_exact_fix", "p5_10_xoshiro_reduced.json"), 30),
+                           ("p5_10_k4_adaptive.json", None), ("p5_10_k5_damped.json", None)):
         ref = json.load(open(os.path.join(src_dir, name)))
         for cand in ref["candidates"]:
             if cand["candidate"] != candidate:
@@ -96,6 +98,7 @@ def ty(src_dir, candidate="TY"):
                     "n_basis": rec["n_basis"], "iterations_run": rec["iterations_run"],
                     "sigma_fs_identity": rec["sigma_fs_identity"], "sigma_final": rec["sigma_final"],
                     "final_donaldson_residual": rec["final_donaldson_residual"],
+                    "elapsed_s": rec.get("elapsed_s"), "source_file": name,
                 })
     gold = json.load(open(os.path.join(src_dir, os.pardir, "tests", "data", "p5_10_determinism_golden.json")))
     f64 = lambda b: struct.unpack("<d", struct.pack("<Q", b))[0]

@@ -238,3 +238,24 @@ def test_metric_cache_round_trip_and_guards(ty, tmp_path):
     s1, so1, sp1 = ty.load_or_solve(root, scfg)
     s2, so2, sp2 = ty.load_or_solve(root, scfg)
     assert so1 == "miss" and so2 == "hit" and sp1 != p1 and np.array_equal(s1["balanced_h"], s2["balanced_h"])
+
+
+def test_k4_adaptive_solves_match_the_reference_records(ty):
+    """Tian-Yau k = 4 at 40,000 points with the reference's adaptive damping (p5_10_k4_adaptive.json: 20 seeds,
+    27-28 iterations, sigma_final 0.27-0.29): the device sampler + solve for three of its seeds."""
+    import json
+    import os
+
+    kat = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "ty_kat.json")))
+    recs = [r for r in kat["records"] if r["k"] == 4]
+    assert len(recs) == 20
+    its = np.array([r["iterations_run"] for r in recs])
+    sf = np.array([r["sigma_final"] for r in recs])
+    sfs = np.array([r["sigma_fs_identity"] for r in recs])
+    got = [ty.solve_ty_metric(ty.TyMetricConfig(k_degree=4, n_sample=40000, max_iter=100, donaldson_tol=1e-6,
+                                                seed=r["seed"])) for r in recs[:3]]
+    for g in got:
+        assert g["n_basis"] == 200 and g["final_donaldson_residual"] < 1e-6
+        assert its.min() - 2 <= g["iterations_run"] <= its.max() + 2
+        assert sf.min() - 3 * sf.std() <= g["sigma_final"] <= sf.max() + 3 * sf.std()
+        assert sfs.min() - 3 * sfs.std() <= g["sigma_fs_identity"] <= sfs.max() + 3 * sfs.std()

@@ -17,13 +17,14 @@ KAT = json.load(open(os.path.join(HERE, "golden", "schoen_kat.json")))
 D = (3, 3, 1)
 
 
-def _records(n_pts):
-    return [r for r in KAT["records"] if r["n_pts"] == n_pts]
+def _records(n_pts, k=3):
+    return [r for r in KAT["records"] if r["n_pts"] == n_pts and r["k"] == k]
 
 
 def test_basis_size_matches_records():
-    b = oracle.schoen_basis(*D)
-    assert {r["n_basis"] for r in KAT["records"]} == {b.shape[0]} == {27}
+    # the reference's tri-degree for each k (schoen_tuple_for_k, src/bin/p5_10_ty_schoen_5sigma.rs:834-842)
+    for k, d, n in ((3, D, 27), (4, (4, 4, 2), 48), (5, (5, 5, 2), 75)):
+        assert {r["n_basis"] for r in KAT["records"] if r["k"] == k} == {oracle.schoen_basis(*d).shape[0]} == {n}
     for d in (D, (2, 2, 1), (4, 4, 2)):
         b = oracle.schoen_basis(*d)
         assert (b[:, :3].sum(1) == d[0]).all() and (b[:, 3:6].sum(1) == d[1]).all() and (b[:, 6:].sum(1) == d[2]).all()

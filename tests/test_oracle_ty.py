@@ -19,8 +19,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 KAT = json.load(open(os.path.join(HERE, "golden", "ty_kat.json")))
 
 
-def _records(n_pts):
-    return [r for r in KAT["records"] if r["n_pts"] == n_pts]
+def _records(n_pts, k=3):
+    return [r for r in KAT["records"] if r["n_pts"] == n_pts and r["k"] == k]
 
 
 def test_chacha_core_matches_independent_chacha20():
@@ -53,8 +53,8 @@ def test_basis_size_matches_records():
     # the generators' own leading monomials z0^3, w0^3, z0 w0 are among the reduced basis's
     for e in ([3, 0, 0, 0, 0, 0, 0, 0], [0, 0, 0, 0, 3, 0, 0, 0], [1, 0, 0, 0, 1, 0, 0, 0]):
         assert any((row == e).all() for row in lms)
-    b3 = oracle.ty_basis(3)
-    assert {r["n_basis"] for r in KAT["records"]} == {b3.shape[0]} == {87}
+    for k, n in ((3, 87), (4, 200), (5, 385)):  # every record of each degree
+        assert {r["n_basis"] for r in KAT["records"] if r["k"] == k} == {oracle.ty_basis(k).shape[0]} == {n}
     for k in (1, 2, 3, 4):
         b = oracle.ty_basis(k)
         assert (b[:, :4].sum(1) == k).all() and (b[:, 4:].sum(1) == k).all()
