@@ -85,6 +85,9 @@ cy3q_status cy3q_ty_sigma(cy3q_ty* t, double* sigma, double* eta, long long cap)
 cy3q_status cy3q_ty_solve(cy3q_ty* t, cy3q_ty_result* out, double* sigma_hist, double* res_hist, int hist_cap);
 /* Kernel launches made by the handle so far. */
 cy3q_status cy3q_ty_launch_count(const cy3q_ty* t, uint64_t* n);
+/* Seed of the next cy3q_ty_sample (the handle, its device buffers and the sampler's scratch are reused, as a
+   per-seed loop over one configuration does). */
+cy3q_status cy3q_ty_set_seed(cy3q_ty* t, uint64_t seed);
 
 /*
  * Schoen: the Z/3 x Z/3 quotient of the complete intersection in CP^2 x CP^2 x CP^1 with coordinates

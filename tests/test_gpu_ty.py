@@ -259,3 +259,13 @@ def test_k4_adaptive_solves_match_the_reference_records(ty):
         assert its.min() - 2 <= g["iterations_run"] <= its.max() + 2
         assert sf.min() - 3 * sf.std() <= g["sigma_final"] <= sf.max() + 3 * sf.std()
         assert sfs.min() - 3 * sfs.std() <= g["sigma_fs_identity"] <= sfs.max() + 3 * sfs.std()
+
+
+def test_solve_many_equals_solves_one_at_a_time(ty):
+    cfgs = [ty.TyMetricConfig(k_degree=3, n_sample=2000, max_iter=20, donaldson_tol=1e-6, seed=s) for s in (1, 2, 3)]
+    cfgs.append(ty.SchoenMetricConfig(n_sample=2000, max_iter=10, donaldson_tol=1e-6, seed=4))
+    many = ty.solve_many(cfgs, workers=4)
+    for cfg, m in zip(cfgs, many):
+        one = ty.solve_ty_metric(cfg)
+        assert np.array_equal(one["balanced_h"], m["balanced_h"])
+        assert one["sigma_final"] == m["sigma_final"] and one["iterations_run"] == m["iterations_run"]
