@@ -42,6 +42,10 @@ typedef struct {
                              k >= 4, ty_metric.rs:247-264); otherwise a static alpha in (0, 1] */
   int sigma_every_iter;   /* 1: sigma after every iteration, as the reference's loop does (ty_metric.rs:686) */
   int device;             /* CUDA device ordinal */
+  const char* checkpoint_path;  /* NULL, or a file rewritten after every iteration of cy3q_ty_solve in the
+                                   reference's checkpoint JSON (write_checkpoint, ty_metric.rs:2603-2656:
+                                   n_basis, iterations, h_re, h_im, donaldson_history, sigma_history; values
+                                   as Rust's {:.17e}; temporary file renamed into place) */
 } cy3q_ty_config;
 
 typedef struct {
@@ -110,6 +114,7 @@ typedef struct {
                                  schoen_metric.rs:649-665); otherwise a static alpha */
   int sigma_every_iter;
   int device;
+  const char* checkpoint_path;  /* as in cy3q_ty_config (schoen_metric.rs:1035-1037) */
 } cy3q_schoen_config;
 
 /* SchoenMetricConfig defaults with the Cy3MetricSpec::Schoen overrides (cy3_metric_unified.rs:289-320). */

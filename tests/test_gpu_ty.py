@@ -269,3 +269,21 @@ def test_solve_many_equals_solves_one_at_a_time(ty):
         one = ty.solve_ty_metric(cfg)
         assert np.array_equal(one["balanced_h"], m["balanced_h"])
         assert one["sigma_final"] == m["sigma_final"] and one["iterations_run"] == m["iterations_run"]
+
+
+def test_checkpoint_file_follows_the_reference_format(ty, tmp_path):
+    """write_checkpoint (ty_metric.rs:2603-2656): rewritten after every iteration with the metric so far."""
+    import json
+
+    path = str(tmp_path / "ty.ckpt.json")
+    cfg = ty.TyMetricConfig(k_degree=3, n_sample=2000, max_iter=6, donaldson_tol=1e-12, seed=9, checkpoint_path=path)
+    r = ty.solve_ty_metric(cfg)
+    d = json.load(open(path))
+    assert set(d) == {"n_basis", "iterations", "h_re", "h_im", "donaldson_history", "sigma_history"}
+    assert d["n_basis"] == 87 and d["iterations"] == r["iterations_run"] == 6
+    N = d["n_basis"]
+    h = (np.array(d["h_re"]) + 1j * np.array(d["h_im"])).reshape(N, N)
+    assert np.array_equal(h, r["balanced_h"])
+    assert d["donaldson_history"] == list(r["donaldson_history"]) and d["sigma_history"] == list(r["sigma_history"])
+    txt = open(path).read()
+    assert "e+" not in txt and "e-0" not in txt  # Rust's {:.17e}: exponent without '+' or leading zeros
