@@ -150,3 +150,17 @@ def test_balanced_sigma_matches_records_at_2000_points():
     ref = np.array([r["sigma_final"] for r in recs])
     got = np.array([m["sigma_final"] for m in mine])
     assert abs(got.mean() / ref.mean() - 1) < 0.1
+
+
+def test_product_bases_equal_the_oracle_bases():
+    """The library's Groebner bases (Buchberger over F_p, host code) against the oracle's (over f64, as the
+    reference computes them): identical monomial lists, in the reference's order."""
+    from papers_b200 import build
+
+    build.build()
+    from papers_b200 import ty
+
+    for k in (1, 2, 3, 4, 5):
+        assert np.array_equal(ty.ty_basis(k), oracle.ty_basis(k))
+    for d in ((3, 3, 1), (2, 2, 1), (4, 4, 2), (5, 5, 2), (3, 3, 2)):
+        assert np.array_equal(ty.schoen_basis(*d), oracle.schoen_basis(*d))
