@@ -287,3 +287,48 @@ def test_checkpoint_file_follows_the_reference_format(ty, tmp_path):
     assert d["donaldson_history"] == list(r["donaldson_history"]) and d["sigma_history"] == list(r["sigma_history"])
     txt = open(path).read()
     assert "e+" not in txt and "e-0" not in txt  # Rust's {:.17e}: exponent without '+' or leading zeros
+
+
+def test_edge_cases_and_failures(ty):
+    # invalid configurations are refused before any device work
+    with pytest.raises(ty.Cy3qError) as e:
+        ty.TyWorkspace(ty.TyMetricConfig(k_degree=0))
+    assert e.value.status == 1
+    with pytest.raises(ty.Cy3qError):
+        ty.TyWorkspace(ty.SchoenMetricConfig(d_x=0, d_y=0, d_t=0))
+    ws = _ws(ty, 3)
+    with pytest.raises(ty.Cy3qError) as e:
+        ws.set_points(np.zeros((0, 16)), np.zeros(0), np.zeros(0))
+    assert e.value.status == 11
+    # zero weights: the sum of weights is not positive, so the iteration fails as the reference's returns NaN
+    # (ty_metric.rs:1151-1156) and h is kept
+    c, om, w, zw = oracle.ty_sample(500, 2)
+    ws.set_points(c, np.abs(om) ** 2, np.zeros_like(w))
+    h0 = ws.h
+    with pytest.raises(ty.Cy3qError) as e:
+        ws.donaldson_step()
+    assert e.value.status == 6 and np.array_equal(ws.h, h0)
+    vals = oracle.ty_sections(c, oracle.ty_basis(3), derivs=False)
+    assert np.isnan(oracle.ty_donaldson_step(vals, np.zeros_like(w), np.eye(ws.n_basis, dtype=complex))[1])
+    # a NaN weight poisons the weight sum the same way; sigma skips the invalid points, as compute_sigma does
+    o2 = np.abs(om) ** 2
+    w2, o22 = w.copy(), o2.copy()
+    w2[:7] = np.nan
+    o22[7:11] = 0.0
+    ws.set_points(c, o22, w2)
+    so, _ = oracle.ty_sigma(c, o22, w2, 3, np.eye(ws.n_basis, dtype=complex))
+    assert _rel(ws.sigma(), so) < 1e-10
+    with pytest.raises(ty.Cy3qError) as e:
+        ws.donaldson_step()
+    assert e.value.status == 6
+    # negative and zero weights enter the normalising sum but not T (the reference's lane guard)
+    w3 = w.copy()
+    w3[:5] = 0.0
+    w3[5:9] = -w3[5:9]
+    ws.set_points(c, o2, w3)
+    ho, ro = oracle.ty_donaldson_step(vals, w3, np.eye(ws.n_basis, dtype=complex))
+    assert _rel(ws.donaldson_step(), ro) < 1e-9
+    assert np.linalg.norm(ws.h - ho) / np.linalg.norm(ho) < 1e-10
+    # a one-point request still samples its 64 lines
+    tiny = ty.TyWorkspace(ty.TyMetricConfig(k_degree=2, n_sample=1, seed=3))
+    assert tiny.sample() == 1
