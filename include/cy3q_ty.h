@@ -89,6 +89,13 @@ cy3q_status cy3q_ty_sigma(cy3q_ty* t, double* sigma, double* eta, long long cap)
 cy3q_status cy3q_ty_solve(cy3q_ty* t, cy3q_ty_result* out, double* sigma_hist, double* res_hist, int hist_cap);
 /* Kernel launches made by the handle so far. */
 cy3q_status cy3q_ty_launch_count(const cy3q_ty* t, uint64_t* n);
+/* adam_refine_sigma_ty (ty_metric.rs:1488-1583; AdamRefineConfig of schoen_metric.rs:115-136): Adam on
+   sigma^2 with the finite-difference gradient over the 2 N^2 real parameters of h (step fd_step), from the
+   handle's h, updated in place.  All N^2 perturbed sigmas of a step are evaluated in one pass (each form is
+   linear in h; the frames do not depend on it).  hist gets the sigma history (the value before each step and
+   after the last), *n_hist its length. */
+cy3q_status cy3q_ty_adam_refine(cy3q_ty* t, int max_iters, double lr, double fd_step, double tol, double* hist,
+                                int cap, int* n_hist);
 /* Seed of the next cy3q_ty_sample (the handle, its device buffers and the sampler's scratch are reused, as a
    per-seed loop over one configuration does). */
 cy3q_status cy3q_ty_set_seed(cy3q_ty* t, uint64_t seed);

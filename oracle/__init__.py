@@ -113,6 +113,8 @@ def lib():
     L.orc_schoen_solve.argtypes = [C.c_int, C.c_int, C.c_int, sz, C.c_int, d, C.c_uint64, _dp, _dp, _dp, C.c_int,
                                    vp, vp, sz]
     L.orc_schoen_solve.restype = C.c_int
+    L.orc_cicy_adam_refine.argtypes = [C.c_int, _ip, _dp, _dp, _dp, sz, _dp, _dp, C.c_int, d, d, d, _dp, C.c_int]
+    L.orc_cicy_adam_refine.restype = C.c_int
     _lib = L
     return L
 
@@ -757,3 +759,19 @@ def schoen_solve(d, n_sample: int, max_iter: int, tol: float, seed: int):
     return dict(n_points=int(rec[0]), n_basis=N, iterations_run=int(rec[2]), sigma_fs_identity=rec[3],
                 sigma_final=rec[4], final_donaldson_residual=rec[5], sigma_history=sh[:n].copy(),
                 donaldson_history=rh[:n].copy(), h=(hr + 1j * hi).reshape(N, N))
+
+
+def cicy_adam_refine(geom: str, d, coords, omega_sq, w, h, max_iters=50, lr=1e-3, fd_step=1e-3, tol=1e-6):
+    """adam_refine_sigma_ty (ty_metric.rs:1488) / the Schoen twin: finite-difference Adam on sigma^2.
+    geom "ty" (d = (k,)) or "schoen" (d = (d_x, d_y, d_t)); returns (h, sigma history)."""
+    dd = np.zeros(3, dtype=np.int32)
+    dd[: len(d)] = d
+    hr = np.ascontiguousarray(h.real, dtype=np.float64).copy()
+    hi = np.ascontiguousarray(h.imag, dtype=np.float64).copy()
+    cap = max_iters + 2
+    hist = np.zeros(cap)
+    n = lib().orc_cicy_adam_refine(0 if geom == "ty" else 1, dd, np.ascontiguousarray(coords, dtype=np.float64),
+                                   np.ascontiguousarray(omega_sq, dtype=np.float64),
+                                   np.ascontiguousarray(w, dtype=np.float64), coords.shape[0], hr, hi,
+                                   int(max_iters), float(lr), float(fd_step), float(tol), hist, cap)
+    return hr + 1j * hi, hist[:n].copy()

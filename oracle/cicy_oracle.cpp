@@ -1791,6 +1791,107 @@ int solve_loop(const double* S, const double* w, size_t P, int N, SigmaFn sig, b
   return (int)sh.size();
 }
 
+
+// adam_refine_sigma_ty (TY:1488-1583; the Schoen loop is the same): finite-difference Adam on sigma^2 over the
+// 2 N^2 real parameters of h, each perturbation followed by renormalise_h_trace_ty (TY:1585-1600).
+template <class SigmaFn>
+int fd_adam(SigmaFn sig, int N, double* hr, double* hi, int max_iters, double lr, double eps, double tol,
+            double* hist, int cap) {
+  const size_t NN = (size_t)N * N, nd = 2 * NN;
+  const double b1 = 0.9, b2 = 0.999, ea = 1.0e-8;
+  std::vector<double> m(nd, 0.0), v(nd, 0.0), sr(NN), si(NN), g(nd);
+  auto renorm = [&](double* r, double* i) {
+    double tr = 0.0;
+    for (int a = 0; a < N; ++a) tr += r[(size_t)a * N + a];
+    if (std::fabs(tr) > 1.0e-30) {
+      const double sc = (double)N / tr;
+      for (size_t q = 0; q < NN; ++q) r[q] *= sc;
+      for (size_t q = 0; q < NN; ++q) i[q] *= sc;
+    }
+  };
+  auto powi = [](double a, int b) {
+    double r = 1.0;
+    for (;;) {
+      if (b & 1) r *= a;
+      b /= 2;
+      if (b == 0) break;
+      a *= a;
+    }
+    return r;
+  };
+  int nh = 0, t = 0;
+  double prev = INFINITY;
+  for (int it = 0; it < max_iters; ++it) {
+    std::copy(hr, hr + NN, sr.begin());
+    std::copy(hi, hi + NN, si.begin());
+    const double sb = sig(hr, hi);
+    if (!std::isfinite(sb)) break;
+    if (nh < cap) hist[nh] = sb;
+    ++nh;
+    if (t > 0 && std::isfinite(prev) && prev > 0.0 && (prev - sb) < tol * prev) break;
+    const double sq = sb * sb;
+    std::fill(g.begin(), g.end(), 0.0);
+    for (int a = 0; a < N; ++a)
+      for (int b = 0; b < N; ++b) {
+        std::copy(sr.begin(), sr.end(), hr);
+        std::copy(si.begin(), si.end(), hi);
+        if (a == b)
+          hr[(size_t)a * N + a] += eps;
+        else {
+          hr[(size_t)a * N + b] += eps;
+          hr[(size_t)b * N + a] += eps;
+        }
+        renorm(hr, hi);
+        const double sp = sig(hr, hi);
+        if (std::isfinite(sp)) g[(size_t)a * N + b] = (sp * sp - sq) / eps;
+      }
+    for (int a = 0; a < N; ++a)
+      for (int b = a + 1; b < N; ++b) {
+        std::copy(sr.begin(), sr.end(), hr);
+        std::copy(si.begin(), si.end(), hi);
+        hi[(size_t)a * N + b] += eps;
+        hi[(size_t)b * N + a] -= eps;
+        renorm(hr, hi);
+        const double sp = sig(hr, hi);
+        if (std::isfinite(sp)) g[NN + (size_t)a * N + b] = (sp * sp - sq) / eps;
+      }
+    std::copy(sr.begin(), sr.end(), hr);
+    std::copy(si.begin(), si.end(), hi);
+    ++t;
+    const double bc1 = 1.0 - powi(b1, t), bc2 = 1.0 - powi(b2, t);
+    const double scale = lr * (std::sqrt(bc2) / bc1);
+    for (size_t q = 0; q < NN; ++q) {
+      m[q] = b1 * m[q] + (1.0 - b1) * g[q];
+      v[q] = b2 * v[q] + (1.0 - b2) * g[q] * g[q];
+      hr[q] -= scale * m[q] / (std::sqrt(v[q]) + ea);
+    }
+    for (int a = 0; a < N; ++a)
+      for (int b = a + 1; b < N; ++b) {
+        const double avg = 0.5 * (hr[(size_t)a * N + b] + hr[(size_t)b * N + a]);
+        hr[(size_t)a * N + b] = avg;
+        hr[(size_t)b * N + a] = avg;
+      }
+    for (int a = 0; a < N; ++a)
+      for (int b = a + 1; b < N; ++b) {
+        const size_t q = NN + (size_t)a * N + b;
+        m[q] = b1 * m[q] + (1.0 - b1) * g[q];
+        v[q] = b2 * v[q] + (1.0 - b2) * g[q] * g[q];
+        const double upd = scale * m[q] / (std::sqrt(v[q]) + ea);
+        hi[(size_t)a * N + b] -= upd;
+        hi[(size_t)b * N + a] += upd;
+      }
+    for (int a = 0; a < N; ++a) hi[(size_t)a * N + a] = 0.0;
+    renorm(hr, hi);
+    prev = sb;
+  }
+  const double sf = sig(hr, hi);
+  if (std::isfinite(sf)) {
+    if (nh < cap) hist[nh] = sf;
+    ++nh;
+  }
+  return nh;
+}
+
 }  // namespace
 
 extern "C" {
@@ -2005,6 +2106,24 @@ int orc_schoen_solve(int dx, int dy, int dt, size_t n_sample, int max_iter, doub
   return solve_loop(sd.S.data(), sd.w.data(), sd.pts.size(), N,
                     [&](const double* hr, const double* hi) { return s_sigma(sd, hr, hi, nullptr); },
                     dx + dy + dt >= 10, max_iter, tol, rec, sig_hist, res_hist, hist_cap, h_re, h_im, h_cap);
+}
+
+
+// FD-Adam sigma refinement on points (coords, omega_sq, weight) for geometry 0 (Tian-Yau, degree d[0]) or 1
+// (Schoen, d[0..2]) from (h_re, h_im), updated in place; history [cap]; returns its length.
+int orc_cicy_adam_refine(int geom, const int* d, const double* coords, const double* omega_sq, const double* weight,
+                         size_t P, double* h_re, double* h_im, int max_iters, double lr, double fd_step, double tol,
+                         double* hist, int cap) {
+  if (geom == 0) {
+    TyData td = import_points(coords, omega_sq, weight, P, d[0]);
+    build_sections(td, true);
+    return fd_adam([&](const double* r, const double* i) { return sigma_of(td, r, i, nullptr); },
+                   (int)td.basis.size(), h_re, h_im, max_iters, lr, fd_step, tol, hist, cap);
+  }
+  SData sd = s_import(coords, omega_sq, weight, P, d[0], d[1], d[2]);
+  s_build(sd);
+  return fd_adam([&](const double* r, const double* i) { return s_sigma(sd, r, i, nullptr); }, (int)sd.basis.size(),
+                 h_re, h_im, max_iters, lr, fd_step, tol, hist, cap);
 }
 
 }  // extern "C"

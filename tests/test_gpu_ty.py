@@ -332,3 +332,27 @@ def test_edge_cases_and_failures(ty):
     # a one-point request still samples its 64 lines
     tiny = ty.TyWorkspace(ty.TyMetricConfig(k_degree=2, n_sample=1, seed=3))
     assert tiny.sample() == 1
+
+
+@pytest.mark.parametrize("geom", ["ty", "schoen"])
+def test_fd_adam_matches_oracle(ty, geom):
+    """adam_refine_sigma_ty on the device (all N^2 perturbed sigmas of a step in one pass) against the oracle's
+    restatement, which re-evaluates sigma from scratch for every perturbation."""
+    if geom == "ty":
+        c, om, w, _ = oracle.ty_sample(300, 3)
+        ws, d = _ws(ty, 2), (2,)
+    else:
+        c, om, w, _ = oracle.schoen_sample(300, 3)
+        ws, d = _sws(ty), D
+    o2 = np.abs(om) ** 2
+    ws.set_points(c, o2, w)
+    N = ws.n_basis
+    rng = np.random.default_rng(1)
+    a = rng.standard_normal((N, N)) + 1j * rng.standard_normal((N, N))
+    h0 = np.eye(N) + 0.02 * (a + a.conj().T)
+    ws.h = h0
+    hist = ws.adam_refine(max_iters=3)
+    ho, hist_o = oracle.cicy_adam_refine(geom, d, c, o2, w, h0, max_iters=3)
+    assert len(hist) == len(hist_o) == 4
+    assert np.abs(hist / hist_o - 1).max() < 1e-9
+    assert np.linalg.norm(ws.h - ho) / np.linalg.norm(ho) < 1e-9

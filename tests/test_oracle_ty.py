@@ -164,3 +164,20 @@ def test_product_bases_equal_the_oracle_bases():
         assert np.array_equal(ty.ty_basis(k), oracle.ty_basis(k))
     for d in ((3, 3, 1), (2, 2, 1), (4, 4, 2), (5, 5, 2), (3, 3, 2)):
         assert np.array_equal(ty.schoen_basis(*d), oracle.schoen_basis(*d))
+
+
+def test_fd_adam_restatement_starts_from_sigma_and_descends():
+    """adam_refine_sigma_ty (ty_metric.rs:1488-1583): the history opens with sigma of the starting h, the
+    Adam steps on sigma^2 lower sigma from the Fubini-Study identity, and h stays Hermitian with trace N."""
+    c, om, w, _ = oracle.ty_sample(300, 3)
+    o2 = np.abs(om) ** 2
+    N = oracle.ty_basis(2).shape[0]
+    h0 = np.eye(N, dtype=complex)
+    s0, _ = oracle.ty_sigma(c, o2, w, 2, h0)
+    h, hist = oracle.cicy_adam_refine("ty", (2,), c, o2, w, h0, max_iters=3)
+    assert len(hist) == 4 and abs(hist[0] / s0 - 1) < 1e-12
+    assert (np.diff(hist) < 0).all()
+    s1, _ = oracle.ty_sigma(c, o2, w, 2, h)
+    assert abs(hist[-1] / s1 - 1) < 1e-12
+    assert np.abs(h - h.conj().T).max() < 1e-12
+    assert abs(np.trace(h).real - N) < 1e-9
