@@ -63,7 +63,7 @@ def parse():
 # clocks during the timed region
 # ------------------------------------------------------------------------------------------------
 class ClockSampler:
-    """SM clock and clock-event reasons of this process's GPU, sampled every 5 ms through NVML (the GPU found by
+    """SM clock and clock-event reasons of this process's GPU, sampled every 1 ms through NVML (the GPU found by
     its UUID, so the index does not depend on CUDA_VISIBLE_DEVICES); nvidia-smi at 200 ms when NVML is not
     available.  Reasons are kept when they were active in any sample."""
 
@@ -113,7 +113,7 @@ class ClockSampler:
                                      int(pynvml.nvmlDeviceGetCurrentClocksEventReasons(h))))
             except Exception:
                 pass
-            time.sleep(0.005)
+            time.sleep(0.001)
 
     def _read(self):
         for line in self.proc.stdout:
@@ -131,7 +131,7 @@ class ClockSampler:
             sm = [c for c, _ in self.samples]
             reasons = sorted({nm for _, r in self.samples for nm, bit in bits.items() if r & bit})
             return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": self.smax, "reasons": reasons,
-                    "samples": len(sm), "source": "nvml, 5 ms"}
+                    "samples": len(sm), "source": "nvml, 1 ms"}
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.proc.terminate()
@@ -600,7 +600,7 @@ def main():
     s.h_block = np.eye(2 * N)
 
     # ---- timed region: K balancing iterations, device-timed (the production path: each step's body is
-    # replayed from a CUDA graph).  The clock record is sampled every 5 ms from just before the timed
+    # replayed from a CUDA graph).  The clock record is sampled every 1 ms from just before the timed
     # region to its end (one 20-iteration solve at this workload takes about 25 ms) ----
     clk = ClockSampler(dev)
     s.launch_count(reset=True)
