@@ -739,8 +739,8 @@ def main():
     traffic_per_point, traffic_src = (traffic_from_csv(a.traffic_csv, a.traffic_points) if a.traffic_csv
                                       else (None, None))
     if traffic_per_point is None:
-        traffic_per_point = {"bergman": (206.009856e6 + 121.594112e6) / 100096,
-                             "toperator": (198.705152e6 + 4.694784e6) / 100096}
+        traffic_per_point = {"bergman": (205.269504e6 + 121.626112e6) / 100096,
+                             "toperator": (191.440640e6 + 13.993472e6) / 100096}
         traffic_src = "DRAM bytes per launch scaled from the 100,096-point ncu capture of these kernels"
     cand = {k: v for k, v in stages.items() if k in stage_flops}
     dname, (dms, dcalls) = max(cand.items(), key=lambda kv: kv[1][0]) if cand else ("toperator", (ms, a.steps))
