@@ -238,6 +238,9 @@ typedef struct {
   uint64_t hbm_in_use, hbm_peak;
 } cy3q_server_stats;
 
+/* hbm_budget_bytes: admission limit for the solves in flight (0: 85 % of the free device memory).  The server
+   grows the device's default memory pool to the budget at creation, so that its solves allocate from memory
+   already mapped; cy3q_server_destroy synchronises the device and trims the pool back. */
 cy3q_status cy3q_server_create(int32_t device, uint64_t hbm_budget_bytes, int32_t max_active, cy3q_server** out);
 void cy3q_server_destroy(cy3q_server* srv);
 cy3q_status cy3q_submit(cy3q_server* srv, const cy3q_request* req, uint64_t* ticket);
